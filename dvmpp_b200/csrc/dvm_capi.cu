@@ -1,0 +1,1252 @@
+// Host runtime and C ABI of libdvm_cuda.so (declared in include/dvm_cuda.h).
+//
+// A dvm_ctx owns one stream on one device, a table of simulation descriptors
+// in device memory, an HBM budget, and a grow-only workspace shared by all
+// batched launches.  A dvm_sim is one slab (one cudaMalloc) holding its blob
+// arrays, body data and solver matrices.  Steps of any set of simulations are
+// issued as one sequence of batched kernels (dvm_step_batch), optionally
+// captured once in a CUDA graph and replayed.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dvm_cuda.h"
+#include "dvm_internal.h"
+
+using namespace dvmk;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<uint64_t> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(DVM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+constexpr int kTableCap = 4096;
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int nbody_chunks(uint32_t cap) {
+    const int c = (int)((cap + 65535) / 65536);
+    return std::max(1, std::min(16, c));
+}
+
+}  // namespace
+
+struct SubList {
+    std::vector<int> slots;
+    ListEntry* d_list = nullptr;
+    int n = 0;
+    int max_np = 0;
+    uint64_t total = 0;  // sum of capacities
+};
+
+struct Plan {
+    std::vector<int> slots;            // the batch, in launch order
+    SubList all, euler, rk3, rk3_f32, rk3_f64, eul_f32, eul_f64, refl, del;
+    uint64_t ws_need_cap = 0;          // sizing inputs
+    uint64_t part_elems = 0, rhs_elems = 0, circ_elems = 0;
+    bool need_delete = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t ws_generation = 0;
+    uint64_t launches_per_step = 0;
+    bool warmed = false;  // one eager step issued (kernel attributes set, buffers touched)
+};
+
+struct dvm_ctx {
+    int device = 0;
+    int sms = 148;
+    int cc_major = 0, cc_minor = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0, in_use = 0;
+    InstDesc* d_table = nullptr;
+    InstState* d_state = nullptr;
+    std::vector<dvm_sim*> slots;  // index = table slot
+    uint32_t next_uid = 1;
+    // shared workspace
+    Workspace ws;
+    uint64_t ws_cap = 0, ws_part = 0, ws_rhs = 0, ws_circ = 0, ws_lists = 0;
+    bool ws_delete = false;
+    void* ws_block = nullptr;
+    uint64_t ws_generation = 0;
+    uint64_t ws_bytes = 0;
+    // raw plugin-call scratch
+    void* raw_block = nullptr;
+    size_t raw_bytes = 0;
+    std::map<std::vector<int>, Plan*> plans;
+    std::mutex mu;
+    // CUDA-event profiling of kernel families on the ctx stream (eager steps only)
+    bool profiling = false;
+    struct Rec {
+        int fam;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> pending;
+    std::vector<cudaEvent_t> pool;
+    double prof_ms[DVM_PROF_FAMILIES] = {};
+    uint64_t prof_n[DVM_PROF_FAMILIES] = {};
+};
+
+struct dvm_sim {
+    dvm_ctx* ctx = nullptr;
+    int slot = -1;
+    dvm_sim_params p{};
+    InstDesc h{};        // host copy of the descriptor in the table
+    void* slab = nullptr;
+    uint64_t bytes = 0;
+    double* uniforms = nullptr;  // inject buffer (inside the slab)
+    uint64_t ucap = 0;
+    uint64_t consumed_base = 0;  // uniforms discarded by compaction
+    // host-side panel data (reference geometry, src/VortexSheet.cpp:78-102)
+    std::vector<double> xc, zc, ds, theta, enx, enz;
+};
+
+namespace {
+
+// ---- plans ------------------------------------------------------------------------
+void free_plan(Plan* pl) {
+    if (!pl) return;
+    if (pl->exec) cudaGraphExecDestroy(pl->exec);
+    if (pl->graph) cudaGraphDestroy(pl->graph);
+    SubList* subs[] = {&pl->all, &pl->euler, &pl->rk3, &pl->rk3_f32, &pl->rk3_f64,
+                       &pl->eul_f32, &pl->eul_f64, &pl->refl, &pl->del};
+    for (SubList* s : subs)
+        if (s->d_list) cudaFree(s->d_list);
+    delete pl;
+}
+
+void drop_plans_with(dvm_ctx* c, int slot) {
+    for (auto it = c->plans.begin(); it != c->plans.end();) {
+        if (slot < 0 || std::find(it->first.begin(), it->first.end(), slot) != it->first.end()) {
+            free_plan(it->second);
+            it = c->plans.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
+int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl) {
+    sl.n = (int)sl.slots.size();
+    if (sl.n == 0) return DVM_OK;
+    std::vector<ListEntry> h(sl.n);
+    uint64_t coff = 0, poff = 0, roff = 0, cofs = 0;
+    for (int k = 0; k < sl.n; ++k) {
+        const dvm_sim* s = c->slots[sl.slots[k]];
+        ListEntry& e = h[k];
+        std::memset(&e, 0, sizeof(e));
+        e.inst = s->slot;
+        e.cap = s->h.cap;
+        e.chunks = nbody_chunks(e.cap);
+        e.rhs_chunks = (int)std::max<uint64_t>(1, (e.cap + kAtChunk - 1) / kAtChunk);
+        e.npad = (int)align_up((size_t)s->h.np, 256);
+        e.coff = coff;
+        e.poff = poff;
+        e.roff = roff;
+        e.cofs = cofs;
+        coff += e.cap;  // caps are multiples of kCapAlign
+        poff += (uint64_t)e.chunks * e.cap;
+        roff += (uint64_t)e.rhs_chunks * e.npad;
+        cofs += (uint64_t)e.rhs_chunks;
+        sl.max_np = std::max(sl.max_np, s->h.np);
+    }
+    sl.total = coff;
+    pl.ws_need_cap = std::max(pl.ws_need_cap, coff);
+    pl.part_elems = std::max(pl.part_elems, poff);
+    pl.rhs_elems = std::max(pl.rhs_elems, roff);
+    pl.circ_elems = std::max(pl.circ_elems, cofs);
+    CK(cudaMalloc(&sl.d_list, sizeof(ListEntry) * sl.n));
+    CK(cudaMemcpy(sl.d_list, h.data(), sizeof(ListEntry) * sl.n, cudaMemcpyHostToDevice));
+    return DVM_OK;
+}
+
+int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint64_t circ,
+                     int nlist, bool need_delete) {
+    if (cap <= c->ws_cap && part <= c->ws_part && rhs <= c->ws_rhs && circ <= c->ws_circ &&
+        (uint64_t)nlist <= c->ws_lists && (!need_delete || c->ws_delete))
+        return DVM_OK;
+    cap = std::max<uint64_t>({cap, c->ws_cap, kCapAlign});
+    part = std::max(part, c->ws_part);
+    rhs = std::max(rhs, c->ws_rhs);
+    circ = std::max(circ, c->ws_circ);
+    const uint64_t lists = std::max<uint64_t>({(uint64_t)nlist, c->ws_lists, 64});
+    need_delete = need_delete || c->ws_delete;
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->ws_block) {
+        cudaFree(c->ws_block);
+        c->in_use -= c->ws_bytes;
+        c->ws_block = nullptr;
+    }
+    const size_t cub = cub_sort_bytes(cap);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        return o;
+    };
+    const size_t o_keys_in = take(8 * cap), o_keys_out = take(8 * cap), o_vals = take(4 * cap),
+                 o_perm = take(4 * cap), o_packed = take(32 * cap),
+                 o_meta = take(sizeof(TileMeta) * (cap / kBsST + 1)), o_part = take(16 * part),
+                 o_rhs = take(16 * rhs), o_circ = take(8 * circ + 8), o_cub = take(cub + 256),
+                 o_work = take(64 * sizeof(unsigned)), o_flags = take(cap),
+                 o_tiles = take(4 * (cap / 1024 + 1)),
+                 o_comp = need_delete ? take(8 * 8 * cap) : take(8),
+                 o_jobs = take(256 * lists);
+    const uint64_t bytes = off;
+    if (c->in_use + bytes > c->budget)
+        return fail(DVM_ERR_OOM, "workspace of " + std::to_string(bytes) +
+                                     " B exceeds the HBM budget");
+    void* blk = nullptr;
+    CK(cudaMalloc(&blk, bytes));
+    c->ws_block = blk;
+    c->ws_bytes = bytes;
+    c->in_use += bytes;
+    char* b = static_cast<char*>(blk);
+    Workspace& w = c->ws;
+    w.total_cap = cap;
+    w.keys_in = reinterpret_cast<uint64_t*>(b + o_keys_in);
+    w.keys_out = reinterpret_cast<uint64_t*>(b + o_keys_out);
+    w.vals_in = reinterpret_cast<uint32_t*>(b + o_vals);
+    w.perm = reinterpret_cast<uint32_t*>(b + o_perm);
+    w.packed = reinterpret_cast<double4*>(b + o_packed);
+    w.meta = reinterpret_cast<TileMeta*>(b + o_meta);
+    w.part = reinterpret_cast<double2*>(b + o_part);
+    w.rhs_part = reinterpret_cast<double2*>(b + o_rhs);
+    w.circ_part = reinterpret_cast<double*>(b + o_circ);
+    w.cub_tmp = b + o_cub;
+    w.cub_bytes = cub;
+    w.work = reinterpret_cast<unsigned*>(b + o_work);
+    w.flags = reinterpret_cast<uint8_t*>(b + o_flags);
+    w.tile_counts = reinterpret_cast<uint32_t*>(b + o_tiles);
+    w.compact = need_delete ? reinterpret_cast<double*>(b + o_comp) : nullptr;
+    w.jobs = b + o_jobs;
+    c->ws_cap = cap;
+    c->ws_part = part;
+    c->ws_rhs = rhs;
+    c->ws_circ = circ;
+    c->ws_lists = lists;
+    c->ws_delete = need_delete;
+    c->ws_generation++;
+    return DVM_OK;
+}
+
+int key_bits_for(int nlist) {
+    int b = 1;
+    while ((1 << b) < nlist) ++b;
+    return 32 + b;
+}
+
+// Profiling helpers: an event pair around a kernel family on the ctx stream.
+int prof_begin(dvm_ctx* c, int fam) {
+    if (!c->profiling) return -1;
+    cudaEvent_t a, b;
+    if (c->pool.size() >= 2) {
+        a = c->pool.back();
+        c->pool.pop_back();
+        b = c->pool.back();
+        c->pool.pop_back();
+    } else {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    cudaEventRecord(a, c->stream);
+    c->pending.push_back({fam, a, b});
+    return (int)c->pending.size() - 1;
+}
+
+void prof_end(dvm_ctx* c, int idx) {
+    if (idx < 0) return;
+    cudaEventRecord(c->pending[idx].b, c->stream);
+}
+
+void prof_fold(dvm_ctx* c) {
+    if (c->pending.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (auto& r : c->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            c->prof_ms[r.fam] += ms;
+            c->prof_n[r.fam] += 1;
+        }
+        c->pool.push_back(r.a);
+        c->pool.push_back(r.b);
+    }
+    c->pending.clear();
+}
+
+// Issue one step of every simulation in the plan (no synchronisation).
+void issue_step(dvm_ctx* c, Plan& pl) {
+    cudaStream_t s = c->stream;
+    InstDesc* T = c->d_table;
+    InstState* S = c->d_state;
+    Workspace ws = c->ws;
+    const int sms = c->sms;
+    uint64_t L = 0;
+    auto on = [&](const SubList& sl) {
+        ws.total_cap = sl.total;
+        ws.key_bits = key_bits_for(sl.n);
+        return ws;
+    };
+    auto nbody = [&](SubList& sl, int prec) {
+        if (!sl.n) return;
+        on(sl);
+        int p = prof_begin(c, DVM_PROF_SORT);
+        biot_savart_prepare(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        prof_end(c, p);
+        p = prof_begin(c, DVM_PROF_NBODY);
+        biot_savart_compute(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        prof_end(c, p);
+        p = prof_begin(c, DVM_PROF_SORT);
+        biot_savart_finish(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        prof_end(c, p);
+        L += (prec == kF32) ? 4 : 3;
+        p = prof_begin(c, DVM_PROF_RHS);
+        sheet_rhs(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        prof_end(c, p);
+        L += 3;
+    };
+    auto stage = [&](SubList& g, int mode) {
+        on(g);
+        int p = prof_begin(c, DVM_PROF_SOLVE);
+        sheet_solve(T, S, g.d_list, g.n, g.max_np, s);
+        prof_end(c, p);
+        p = prof_begin(c, DVM_PROF_SHEETVEL);
+        sheet_velocity(T, S, g.d_list, g.n, mode, g.max_np, ws, sms, s);
+        prof_end(c, p);
+        L += 4;
+    };
+    const int pstep = prof_begin(c, DVM_PROF_STEP);
+    int p = prof_begin(c, DVM_PROF_LOADS);
+    step_counter(S, pl.all.d_list, pl.all.n, s);
+    prof_end(c, p);
+    L += 1;
+    if (pl.euler.n) {
+        nbody(pl.eul_f32, kF32);
+        nbody(pl.eul_f64, kF64);
+        stage(pl.euler, 1);
+    }
+    if (pl.rk3.n) {
+        for (int st = 0; st < 3; ++st) {
+            nbody(pl.rk3_f32, kF32);
+            nbody(pl.rk3_f64, kF64);
+            stage(pl.rk3, 2 + st);
+        }
+    }
+    on(pl.all);
+    p = prof_begin(c, DVM_PROF_DIFFREL);
+    diffuse(T, S, pl.all.d_list, pl.all.n, ws, sms, s);
+    release(T, S, pl.all.d_list, pl.all.n, pl.all.max_np, s);
+    prof_end(c, p);
+    L += 2;
+    if (pl.refl.n) {
+        on(pl.refl);
+        p = prof_begin(c, DVM_PROF_CROSS);
+        reflect(T, S, pl.refl.d_list, pl.refl.n, pl.refl.max_np, ws, sms, s);
+        prof_end(c, p);
+        L += 1;
+    }
+    if (pl.del.n) {
+        on(pl.del);
+        p = prof_begin(c, DVM_PROF_CROSS);
+        delete_inside(T, S, pl.del.d_list, pl.del.n, pl.del.max_np, ws, sms, s);
+        prof_end(c, p);
+        L += 4;
+    }
+    p = prof_begin(c, DVM_PROF_LOADS);
+    loads(T, S, pl.all.d_list, pl.all.n, pl.all.max_np, s);
+    prof_end(c, p);
+    prof_end(c, pstep);
+    L += 1;
+    pl.launches_per_step = L;
+}
+
+int get_plan(dvm_ctx* c, const std::vector<int>& slots, Plan** out) {
+    auto it = c->plans.find(slots);
+    if (it != c->plans.end()) {
+        *out = it->second;
+        return DVM_OK;
+    }
+    Plan* pl = new Plan();
+    pl->slots = slots;
+    for (int sl : slots) {
+        const dvm_sim* s = c->slots[sl];
+        pl->all.slots.push_back(sl);
+        const bool rk3 = s->h.scheme == kRK3, f32 = s->h.precision == kF32;
+        (rk3 ? pl->rk3 : pl->euler).slots.push_back(sl);
+        if (rk3) (f32 ? pl->rk3_f32 : pl->rk3_f64).slots.push_back(sl);
+        else (f32 ? pl->eul_f32 : pl->eul_f64).slots.push_back(sl);
+        if (s->h.cross == kDelete) {
+            pl->del.slots.push_back(sl);
+            pl->need_delete = true;
+        } else {
+            pl->refl.slots.push_back(sl);
+        }
+    }
+    SubList* subs[] = {&pl->all, &pl->euler, &pl->rk3, &pl->rk3_f32, &pl->rk3_f64,
+                       &pl->eul_f32, &pl->eul_f64, &pl->refl, &pl->del};
+    for (SubList* s : subs) {
+        const int rc = build_sublist(c, *s, *pl);
+        if (rc) {
+            free_plan(pl);
+            return rc;
+        }
+    }
+    c->plans[slots] = pl;
+    *out = pl;
+    return DVM_OK;
+}
+
+int upload_desc(dvm_sim* s) {
+    CK(cudaMemcpyAsync(s->ctx->d_table + s->slot, &s->h, sizeof(InstDesc), cudaMemcpyHostToDevice,
+                       s->ctx->stream));
+    return DVM_OK;
+}
+
+int check_device_status(dvm_sim* s) {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, &s->ctx->d_state[s->slot].status, sizeof(int), cudaMemcpyDeviceToHost,
+                       s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return st;
+}
+
+int run_steps(dvm_ctx* c, const std::vector<int>& slots, int nsteps, bool use_graph) {
+    Plan* pl = nullptr;
+    int rc = get_plan(c, slots, &pl);
+    if (rc) return rc;
+    rc = ensure_workspace(c, pl->ws_need_cap, pl->part_elems, pl->rhs_elems, pl->circ_elems,
+                          (int)slots.size(), pl->need_delete);
+    if (rc) return rc;
+    if (pl->exec && pl->ws_generation != c->ws_generation) {
+        cudaGraphExecDestroy(pl->exec);
+        cudaGraphDestroy(pl->graph);
+        pl->exec = nullptr;
+        pl->graph = nullptr;
+    }
+    if (c->profiling) use_graph = false;  // events are recorded around eager launches
+    for (int k = 0; k < nsteps; ++k) {
+        if (use_graph && pl->exec) {
+            CK(cudaGraphLaunch(pl->exec, c->stream));
+            g_launches += pl->launches_per_step;
+            continue;
+        }
+        if (use_graph && pl->warmed) {  // capture only after one eager step of this plan
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            issue_step(c, *pl);
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamEndCapture(c->stream, &g));
+            cudaGraphExec_t ex = nullptr;
+            CK(cudaGraphInstantiate(&ex, g, 0));
+            pl->graph = g;
+            pl->exec = ex;
+            pl->ws_generation = c->ws_generation;
+            CK(cudaGraphLaunch(pl->exec, c->stream));
+            g_launches += pl->launches_per_step;
+            continue;
+        }
+        issue_step(c, *pl);
+        CK(cudaGetLastError());
+        pl->warmed = true;
+        g_launches += pl->launches_per_step;
+    }
+    CK(cudaGetLastError());
+    return DVM_OK;
+}
+
+// Reference panel geometry on the host, in FP64 with the C library's functions
+// (src/VortexSheet.cpp:74, 78-102); O(np) once per body.
+void host_geometry(dvm_sim* s, const double* xp, const double* zp, int npts) {
+    const int np = npts - 1;
+    s->xc.resize(np);
+    s->zc.resize(np);
+    s->ds.resize(np);
+    s->theta.resize(np);
+    s->enx.resize(np);
+    s->enz.resize(np);
+    for (int i = 0; i < np; ++i) {
+        s->xc[i] = 0.5 * (xp[i] + xp[i + 1]);
+        s->zc[i] = 0.5 * (zp[i] + zp[i + 1]);
+        const double dx = xp[i + 1] - xp[i];
+        const double dz = zp[i + 1] - zp[i];
+        s->ds[i] = std::sqrt(std::pow(dx, 2.0) + std::pow(dz, 2.0));
+        s->theta[i] = std::atan2(dz, dx);
+        s->enx[i] = dz / s->ds[i];
+        s->enz[i] = -dx / s->ds[i];
+    }
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+int dvm_abi_version(void) { return DVM_ABI_VERSION; }
+
+const char* dvm_status_string(int status) {
+    switch (status) {
+        case DVM_OK: return "ok";
+        case DVM_ERR_ARG: return "bad argument";
+        case DVM_ERR_OOM: return "out of device memory / HBM budget";
+        case DVM_ERR_CUDA: return "CUDA error";
+        case DVM_ERR_TIMEOUT: return "device wait timed out";
+        case DVM_ERR_CAPACITY: return "blob capacity exceeded";
+        case DVM_ERR_RELEASE: return "negative PanelNewVort in release";
+        case DVM_ERR_STATE: return "invalid state";
+        case DVM_ERR_RNG: return "injected random stream exhausted";
+        case DVM_ERR_NO_DEVICE: return "no usable CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* dvm_last_error(void) { return g_err.c_str(); }
+
+int dvm_ctx_create(int device, uint64_t budget, dvm_ctx** out) {
+    if (!out) return fail(DVM_ERR_ARG, "out is null");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(DVM_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(DVM_ERR_ARG, "bad device index");
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(DVM_ERR_NO_DEVICE, "library is built for sm_100a only");
+    auto* c = new dvm_ctx();
+    c->device = device;
+    c->sms = prop.multiProcessorCount;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = budget ? budget : (uint64_t)(0.9 * (double)fr);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_table, sizeof(InstDesc) * kTableCap);
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_state, sizeof(InstState) * kTableCap);
+    if (e == cudaSuccess) e = cudaMemset(c->d_state, 0, sizeof(InstState) * kTableCap);
+    if (e != cudaSuccess) {
+        dvm_ctx_destroy(c);
+        return fail(DVM_ERR_CUDA, std::string("ctx create: ") + cudaGetErrorString(e));
+    }
+    c->slots.assign(kTableCap, nullptr);
+    c->in_use = 2 * sizeof(InstDesc) * kTableCap;
+    *out = c;
+    return DVM_OK;
+}
+
+int dvm_ctx_destroy(dvm_ctx* c) {
+    if (!c) return DVM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (dvm_sim* s : c->slots)
+        if (s) {
+            cudaFree(s->slab);
+            delete s;
+        }
+    drop_plans_with(c, -1);
+    for (auto& r : c->pending) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    if (c->ws_block) cudaFree(c->ws_block);
+    if (c->raw_block) cudaFree(c->raw_block);
+    if (c->d_table) cudaFree(c->d_table);
+    if (c->d_state) cudaFree(c->d_state);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return DVM_OK;
+}
+
+int dvm_ctx_synchronize(dvm_ctx* c) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    CK(cudaStreamSynchronize(c->stream));
+    return DVM_OK;
+}
+
+int dvm_ctx_memory(dvm_ctx* c, uint64_t* in_use, uint64_t* budget) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    if (in_use) *in_use = c->in_use;
+    if (budget) *budget = c->budget;
+    return DVM_OK;
+}
+
+int dvm_ctx_device_info(dvm_ctx* c, int* sms, int* ma, int* mi) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    if (sms) *sms = c->sms;
+    if (ma) *ma = c->cc_major;
+    if (mi) *mi = c->cc_minor;
+    return DVM_OK;
+}
+
+int dvm_ctx_set_profiling(dvm_ctx* c, int on) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->profiling = on != 0;
+    return DVM_OK;
+}
+
+int dvm_ctx_profile(dvm_ctx* c, int fam, double* ms, uint64_t* n) {
+    if (!c || fam < 0 || fam >= DVM_PROF_FAMILIES) return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    prof_fold(c);
+    if (ms) *ms = c->prof_ms[fam];
+    if (n) *n = c->prof_n[fam];
+    return DVM_OK;
+}
+
+int dvm_ctx_profile_reset(dvm_ctx* c) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    std::lock_guard<std::mutex> lk(c->mu);
+    prof_fold(c);
+    for (int f = 0; f < DVM_PROF_FAMILIES; ++f) {
+        c->prof_ms[f] = 0.0;
+        c->prof_n[f] = 0;
+    }
+    return DVM_OK;
+}
+
+int dvm_ctx_launch_count(dvm_ctx* c, uint64_t* n) {
+    if (!c || !n) return fail(DVM_ERR_ARG, "null argument");
+    *n = g_launches.load();
+    return DVM_OK;
+}
+
+// Slab layout of one simulation (doubles unless noted; each array 256-B aligned).
+static uint64_t sim_layout(const dvm_sim_params* p, int np, uint64_t cap,
+                           std::vector<size_t>* offs) {
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t o = off;
+        off = align_up(off + bytes, 256);
+        if (offs) offs->push_back(o);
+        return o;
+    };
+    for (int a = 0; a < 10; ++a) take(8 * cap);  // x z circ sigma u w uvs wvs q1 q2
+    take(4 * cap);                               // id
+    take(8 * (np + 1));                          // xp
+    take(8 * (np + 1));                          // zp
+    for (int a = 0; a < 14; ++a) take(8 * np);   // xc zc ds theta enx enz etx etz cth sth c2th s2th psigma gamma
+    take(8 * (size_t)(np + 1) * np);             // A
+    take(8 * (size_t)(np + 1) * np);             // P
+    take(8 * (np + 1));                          // b
+    take(8 * (np + 1));                          // res
+    take(p->rng == DVM_RNG_INJECT ? 8 * std::max<uint64_t>(p->rng_capacity, 1) : 8);
+    return off;
+}
+
+int dvm_sim_bytes(const dvm_sim_params* p, int np, uint64_t* bytes) {
+    if (!p || !bytes || np < 2) return fail(DVM_ERR_ARG, "bad argument");
+    const uint64_t cap = align_up(std::max<uint64_t>(p->capacity, 1), kCapAlign);
+    *bytes = sim_layout(p, np, cap, nullptr);
+    return DVM_OK;
+}
+
+int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const double* bz,
+                   int npts, dvm_sim** out) {
+    if (!c || !p || !bx || !bz || !out) return fail(DVM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (npts < 3) return fail(DVM_ERR_ARG, "body needs at least 3 points (2 panels)");
+    if (p->scheme != DVM_EULER && p->scheme != DVM_RK3) return fail(DVM_ERR_ARG, "bad scheme");
+    if (p->surface_cross < 0 || p->surface_cross > 2) return fail(DVM_ERR_ARG, "bad surface_cross");
+    if (p->precision != DVM_F64 && p->precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
+    if (p->rng != DVM_RNG_INJECT && p->rng != DVM_RNG_PHILOX) return fail(DVM_ERR_ARG, "bad rng");
+    if (!(p->dt > 0) || !(p->nu > 0) || !(p->rho > 0)) return fail(DVM_ERR_ARG, "dt, nu, density must be > 0");
+    if (p->capacity == 0 || p->capacity > 0xF0000000ull) return fail(DVM_ERR_ARG, "bad capacity");
+    const int np = npts - 1;
+    if (np > 2048) return fail(DVM_ERR_ARG, "too many panels (max 2048)");
+    std::lock_guard<std::mutex> lk(c->mu);
+    int slot = -1;
+    for (int i = 1; i < kTableCap; ++i)  // slot 0 is the plugin-call scratch
+        if (!c->slots[i]) {
+            slot = i;
+            break;
+        }
+    if (slot < 0) return fail(DVM_ERR_OOM, "simulation table full");
+    CK(cudaSetDevice(c->device));
+    const uint64_t cap = align_up(p->capacity, kCapAlign);
+    std::vector<size_t> offs;
+    const uint64_t bytes = sim_layout(p, np, cap, &offs);
+    const uint64_t qr_bytes = 8 * (2 * (size_t)np * np + pseudo_inverse_work_doubles(np));
+    if (c->in_use + bytes + qr_bytes > c->budget)
+        return fail(DVM_ERR_OOM, "simulation of " + std::to_string(bytes) +
+                                     " B does not fit the HBM budget");
+    auto* s = new dvm_sim();
+    s->ctx = c;
+    s->slot = slot;
+    s->p = *p;
+    s->bytes = bytes;
+    cudaError_t e = cudaMalloc(&s->slab, bytes);
+    if (e != cudaSuccess) {
+        delete s;
+        return fail(DVM_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    char* b = static_cast<char*>(s->slab);
+    int a = 0;
+    auto nxt = [&]() { return reinterpret_cast<double*>(b + offs[a++]); };
+    InstDesc& h = s->h;
+    std::memset(&h, 0, sizeof(h));
+    h.x = nxt(); h.z = nxt(); h.circ = nxt(); h.sigma = nxt(); h.u = nxt(); h.w = nxt();
+    h.uvs = nxt(); h.wvs = nxt(); h.q1 = nxt(); h.q2 = nxt();
+    h.id = reinterpret_cast<uint32_t*>(nxt());
+    double* xp = nxt();
+    double* zp = nxt();
+    double* xc = nxt(); double* zc = nxt(); double* ds = nxt(); double* th = nxt();
+    double* enx = nxt(); double* enz = nxt(); double* etx = nxt(); double* etz = nxt();
+    double* cth = nxt(); double* sth = nxt(); double* c2 = nxt(); double* s2 = nxt();
+    double* psig = nxt();
+    h.gamma = nxt();
+    double* A = nxt();
+    double* P = nxt();
+    h.b = nxt();
+    h.res = nxt();
+    s->uniforms = nxt();
+    s->ucap = p->rng == DVM_RNG_INJECT ? std::max<uint64_t>(p->rng_capacity, 1) : 0;
+    h.xp = xp; h.zp = zp; h.xc = xc; h.zc = zc; h.ds = ds; h.enx = enx; h.enz = enz;
+    h.etx = etx; h.etz = etz; h.cth = cth; h.sth = sth; h.c2th = c2; h.s2th = s2; h.psigma = psig;
+    h.A = A; h.P = P; h.uniforms = s->uniforms; h.ucount = 0;
+    h.rho = p->rho; h.nu = p->nu; h.dt = p->dt; h.ux = p->ux; h.uz = p->uz;
+    h.cutoff_exp = p->cutoff_exp;
+    h.Ur = std::sqrt(p->ux * p->ux + p->uz * p->uz);  // src/DVMBase.cpp:29
+    h.M = p->max_numpanelvort;
+    h.np = np;
+    h.scheme = p->scheme;
+    h.cross = p->surface_cross;
+    h.rng = p->rng;
+    h.precision = p->precision;
+    h.refine = 1;
+    h.cap = (uint32_t)cap;
+    h.seed = (uint64_t)p->seed;
+    h.uid = 0;  // random streams depend on the seed only, never on the table slot
+    // host geometry (reference arithmetic) and derived per-panel tables
+    host_geometry(s, bx, bz, npts);
+    std::vector<double> vetx(np), vetz(np), vcth(np), vsth(np), vc2(np), vs2(np), vps(np);
+    for (int i = 0; i < np; ++i) {
+        vetx[i] = -s->enz[i];
+        vetz[i] = s->enx[i];
+        vcth[i] = std::cos(s->theta[i]);
+        vsth[i] = std::sin(s->theta[i]);
+        vc2[i] = std::cos(-2.0 * s->theta[i]);
+        vs2[i] = std::sin(-2.0 * s->theta[i]);
+        vps[i] = std::pow(s->ds[i], p->cutoff_exp);  // src/VortexSheet.cpp:325
+    }
+    double xmx = bx[0], xmn = bx[0], zmx = bz[0], zmn = bz[0];
+    for (int i = 1; i < npts; ++i) {
+        xmx = std::max(xmx, bx[i]);
+        xmn = std::min(xmn, bx[i]);
+        zmx = std::max(zmx, bz[i]);
+        zmn = std::min(zmn, bz[i]);
+    }
+    h.area = xmx - xmn;  // src/VortexSheet.cpp:74
+    h.bxmax = xmx + 1e-9 * (1.0 + std::fabs(xmx));
+    h.bzmin = zmn;
+    h.bzmax = zmx;
+    const double L = std::max(xmx - xmn, zmx - zmn);
+    const double cx = 0.5 * (xmx + xmn), cz = 0.5 * (zmx + zmn);
+    h.kx0 = cx - 32.0 * L;
+    h.kz0 = cz - 64.0 * L;
+    h.kinv = 65536.0 / (128.0 * L);
+    auto up = [&](double* d, const double* src, size_t n) {
+        return cudaMemcpyAsync(d, src, 8 * n, cudaMemcpyHostToDevice, c->stream);
+    };
+    e = cudaSuccess;
+    if (e == cudaSuccess) e = up(xp, bx, npts);
+    if (e == cudaSuccess) e = up(zp, bz, npts);
+    if (e == cudaSuccess) e = up(xc, s->xc.data(), np);
+    if (e == cudaSuccess) e = up(zc, s->zc.data(), np);
+    if (e == cudaSuccess) e = up(ds, s->ds.data(), np);
+    if (e == cudaSuccess) e = up(th, s->theta.data(), np);
+    if (e == cudaSuccess) e = up(enx, s->enx.data(), np);
+    if (e == cudaSuccess) e = up(enz, s->enz.data(), np);
+    if (e == cudaSuccess) e = up(etx, vetx.data(), np);
+    if (e == cudaSuccess) e = up(etz, vetz.data(), np);
+    if (e == cudaSuccess) e = up(cth, vcth.data(), np);
+    if (e == cudaSuccess) e = up(sth, vsth.data(), np);
+    if (e == cudaSuccess) e = up(c2, vc2.data(), np);
+    if (e == cudaSuccess) e = up(s2, vs2.data(), np);
+    if (e == cudaSuccess) e = up(psig, vps.data(), np);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h.gamma, 0, 8 * np, c->stream);
+    // influence matrix and pseudo-inverse, once per body
+    double* scratch = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&scratch, qr_bytes);
+    if (e == cudaSuccess) {
+        influence_matrix(xp, zp, xc, zc, ds, th, np, scratch, A, c->stream);
+        pseudo_inverse(A, np, P, scratch, c->stream);
+        g_launches += 2 + 1 + 2 * (uint64_t)np + 1;
+        e = cudaStreamSynchronize(c->stream);
+    }
+    if (scratch) cudaFree(scratch);
+    InstState st0;
+    std::memset(&st0, 0, sizeof(st0));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_state + slot, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_table + slot, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(s->slab);
+        delete s;
+        return fail(DVM_ERR_CUDA, std::string("sim create: ") + cudaGetErrorString(e));
+    }
+    c->slots[slot] = s;
+    c->in_use += bytes;
+    *out = s;
+    return DVM_OK;
+}
+
+int dvm_sim_destroy(dvm_sim* s) {
+    if (!s) return DVM_OK;
+    dvm_ctx* c = s->ctx;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    drop_plans_with(c, s->slot);
+    c->slots[s->slot] = nullptr;
+    c->in_use -= s->bytes;
+    cudaFree(s->slab);
+    delete s;
+    return DVM_OK;
+}
+
+int dvm_sim_set_blobs(dvm_sim* s, uint64_t n, const double* x, const double* z, const double* circ,
+                      const double* sigma) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    if (n > s->h.cap) return fail(DVM_ERR_CAPACITY, "more blobs than the simulation's capacity");
+    if (n && (!x || !z || !circ || !sigma)) return fail(DVM_ERR_ARG, "null blob array");
+    cudaStream_t st = s->ctx->stream;
+    CK(cudaStreamSynchronize(st));
+    if (n) {
+        CK(cudaMemcpyAsync(s->h.x, x, 8 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(s->h.z, z, 8 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(s->h.circ, circ, 8 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(s->h.sigma, sigma, 8 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(s->h.u, 0, 8 * n, st));
+        CK(cudaMemsetAsync(s->h.w, 0, 8 * n, st));
+        CK(cudaMemsetAsync(s->h.uvs, 0, 8 * n, st));
+        CK(cudaMemsetAsync(s->h.wvs, 0, 8 * n, st));
+        std::vector<uint32_t> ids(n);
+        for (uint64_t i = 0; i < n; ++i) ids[i] = (uint32_t)i;
+        CK(cudaMemcpyAsync(s->h.id, ids.data(), 4 * n, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    const uint32_t n32 = (uint32_t)n;
+    CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].n, &n32, 4, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return DVM_OK;
+}
+
+int dvm_sim_num_blobs(dvm_sim* s, uint64_t* n) {
+    if (!s || !n) return fail(DVM_ERR_ARG, "null argument");
+    uint32_t v = 0;
+    CK(cudaMemcpyAsync(&v, &s->ctx->d_state[s->slot].n, 4, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    *n = v;
+    return DVM_OK;
+}
+
+int dvm_sim_num_panels(dvm_sim* s, int* np) {
+    if (!s || !np) return fail(DVM_ERR_ARG, "null argument");
+    *np = s->h.np;
+    return DVM_OK;
+}
+
+int dvm_sim_get_blobs(dvm_sim* s, uint64_t cap, uint64_t* n_out, double* x, double* z, double* circ,
+                      double* sigma, double* u, double* w, double* uvs, double* wvs, uint32_t* id) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    uint64_t n = 0;
+    int rc = dvm_sim_num_blobs(s, &n);
+    if (rc) return rc;
+    if (n_out) *n_out = n;
+    if (n > cap && (x || z || circ || sigma || u || w || uvs || wvs || id))
+        return fail(DVM_ERR_ARG, "output capacity smaller than the blob count");
+    cudaStream_t st = s->ctx->stream;
+    const double* src[] = {s->h.x, s->h.z, s->h.circ, s->h.sigma, s->h.u, s->h.w, s->h.uvs, s->h.wvs};
+    double* dst[] = {x, z, circ, sigma, u, w, uvs, wvs};
+    for (int a = 0; a < 8; ++a)
+        if (dst[a] && n) CK(cudaMemcpyAsync(dst[a], src[a], 8 * n, cudaMemcpyDeviceToHost, st));
+    if (id && n) CK(cudaMemcpyAsync(id, s->h.id, 4 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return DVM_OK;
+}
+
+int dvm_sim_get_gamma(dvm_sim* s, double* g) {
+    if (!s || !g) return fail(DVM_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(g, s->h.gamma, 8 * s->h.np, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_set_gamma(dvm_sim* s, const double* g) {
+    if (!s || !g) return fail(DVM_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(s->h.gamma, g, 8 * s->h.np, cudaMemcpyHostToDevice, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_get_rhs(dvm_sim* s, double* b) {
+    if (!s || !b) return fail(DVM_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(b, s->h.b, 8 * (s->h.np + 1), cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_get_influence(dvm_sim* s, double* A) {
+    if (!s || !A) return fail(DVM_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(A, s->h.A, 8 * (size_t)(s->h.np + 1) * s->h.np, cudaMemcpyDeviceToHost,
+                       s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_get_panels(dvm_sim* s, double* xc, double* zc, double* ds, double* theta, double* enx,
+                       double* enz) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    const size_t b = 8 * (size_t)s->h.np;
+    if (xc) std::memcpy(xc, s->xc.data(), b);
+    if (zc) std::memcpy(zc, s->zc.data(), b);
+    if (ds) std::memcpy(ds, s->ds.data(), b);
+    if (theta) std::memcpy(theta, s->theta.data(), b);
+    if (enx) std::memcpy(enx, s->enx.data(), b);
+    if (enz) std::memcpy(enz, s->enz.data(), b);
+    return DVM_OK;
+}
+
+int dvm_sim_get_loads(dvm_sim* s, double* fx, double* fz, double* cd, double* cl) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &s->ctx->d_state[s->slot], sizeof(st), cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    if (fx) *fx = st.fx;
+    if (fz) *fz = st.fz;
+    if (cd) *cd = st.cd;
+    if (cl) *cl = st.cl;
+    return DVM_OK;
+}
+
+int dvm_sim_get_step(dvm_sim* s, uint32_t* step) {
+    if (!s || !step) return fail(DVM_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(step, &s->ctx->d_state[s->slot].step, 4, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_push_uniforms(dvm_sim* s, const double* u, uint64_t n) {
+    if (!s || (n && !u)) return fail(DVM_ERR_ARG, "null argument");
+    if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
+    cudaStream_t st = s->ctx->stream;
+    uint64_t cursor = 0;
+    CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    uint64_t count = s->h.ucount;
+    if (count + n > s->ucap) {  // drop the consumed prefix
+        const uint64_t keep = count - cursor;
+        if (keep + n > s->ucap) return fail(DVM_ERR_CAPACITY, "uniform buffer too small");
+        if (keep && cursor)
+            CK(cudaMemcpyAsync(s->uniforms, s->uniforms + cursor, 8 * keep, cudaMemcpyDeviceToDevice, st));
+        s->consumed_base += cursor;
+        count = keep;
+        const uint64_t zero = 0;
+        CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].cursor, &zero, 8, cudaMemcpyHostToDevice, st));
+    }
+    if (n) CK(cudaMemcpyAsync(s->uniforms + count, u, 8 * n, cudaMemcpyHostToDevice, st));
+    s->h.ucount = count + n;
+    int rc = upload_desc(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(st));
+    return DVM_OK;
+}
+
+int dvm_sim_rng_position(dvm_sim* s, uint64_t* consumed, uint64_t* avail) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    uint64_t cursor = 0;
+    CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    if (consumed) *consumed = s->consumed_base + cursor;
+    if (avail) *avail = s->h.ucount - cursor;
+    return DVM_OK;
+}
+
+int dvm_sim_status(dvm_sim* s) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    const int st = check_device_status(s);
+    if (st < 0) return st;
+    switch (st) {
+        case 0: return DVM_OK;
+        case kErrCapacity: return fail(DVM_ERR_CAPACITY, "release exceeded the blob capacity");
+        case kErrRelease:
+            return fail(DVM_ERR_RELEASE,
+                        "VortexSheet::release_nascent_vortices_rw: negative PanelNewVort");
+        case kErrRngExhausted: return fail(DVM_ERR_RNG, "injected uniform stream exhausted");
+        default: return fail(st, "device status " + std::to_string(st));
+    }
+}
+
+int dvm_sim_clear_status(dvm_sim* s) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    const int z = 0;
+    CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].status, &z, 4, cudaMemcpyHostToDevice, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_phase(dvm_sim* s, int phase) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    dvm_ctx* c = s->ctx;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    std::vector<int> one{s->slot};
+    Plan* pl = nullptr;
+    int rc = get_plan(c, one, &pl);
+    if (rc) return rc;
+    rc = ensure_workspace(c, pl->ws_need_cap, pl->part_elems, pl->rhs_elems, pl->circ_elems, 1,
+                          pl->need_delete || phase == DVM_PHASE_DELETE);
+    if (rc) return rc;
+    InstDesc* T = c->d_table;
+    InstState* S = c->d_state;
+    Workspace ws = c->ws;
+    ws.key_bits = key_bits_for(1);
+    ws.total_cap = pl->all.total;
+    cudaStream_t st = c->stream;
+    const ListEntry* L = pl->all.d_list;
+    const int np = s->h.np, prec = s->h.precision;
+    switch (phase) {
+        case DVM_PHASE_BIOTSAVART: biot_savart_self(T, S, L, 1, prec, ws, c->sms, st); break;
+        case DVM_PHASE_SOLVE:
+            sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
+            sheet_solve(T, S, L, 1, np, st);
+            break;
+        case DVM_PHASE_SHEETBC: sheet_velocity(T, S, L, 1, 0, np, ws, c->sms, st); break;
+        case DVM_PHASE_CONVECT:
+            for (int k = 0; k < (s->h.scheme == kRK3 ? 3 : 1); ++k) {
+                biot_savart_self(T, S, L, 1, prec, ws, c->sms, st);
+                sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
+                sheet_solve(T, S, L, 1, np, st);
+                sheet_velocity(T, S, L, 1, s->h.scheme == kRK3 ? 2 + k : 1, np, ws, c->sms, st);
+            }
+            break;
+        case DVM_PHASE_DIFFUSE: diffuse(T, S, L, 1, ws, c->sms, st); break;
+        case DVM_PHASE_RELEASE: release(T, S, L, 1, np, st); break;
+        case DVM_PHASE_CROSS:
+            if (s->h.cross == kDelete) delete_inside(T, S, L, 1, np, ws, c->sms, st);
+            else reflect(T, S, L, 1, np, ws, c->sms, st);
+            break;
+        case DVM_PHASE_LOADS: loads(T, S, L, 1, np, st); break;
+        case DVM_PHASE_INCREMENT: step_counter(S, L, 1, st); break;
+        case DVM_PHASE_REFLECT: reflect(T, S, L, 1, np, ws, c->sms, st); break;
+        case DVM_PHASE_DELETE: delete_inside(T, S, L, 1, np, ws, c->sms, st); break;
+        default: return fail(DVM_ERR_ARG, "bad phase");
+    }
+    g_launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    return DVM_OK;
+}
+
+int dvm_sim_step(dvm_sim* s, int nsteps) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    dvm_sim* one[1] = {s};
+    return dvm_step_batch(s->ctx, one, 1, nsteps, 0);
+}
+
+int dvm_step_batch(dvm_ctx* c, dvm_sim* const* sims, int nsims, int nsteps, int use_graph) {
+    if (!c || (nsims && !sims) || nsims < 0 || nsteps < 0) return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0 || nsteps == 0) return DVM_OK;
+    if (nsims > 1024) return fail(DVM_ERR_ARG, "at most 1024 simulations per batch");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    std::vector<int> slots(nsims);
+    for (int i = 0; i < nsims; ++i) {
+        if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        slots[i] = sims[i]->slot;
+    }
+    return run_steps(c, slots, nsteps, use_graph != 0);
+}
+
+// ---- plugin seam ---------------------------------------------------------------------
+static int raw_reserve(dvm_ctx* c, size_t bytes) {
+    if (bytes <= c->raw_bytes) return DVM_OK;
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->raw_block) {
+        cudaFree(c->raw_block);
+        c->in_use -= c->raw_bytes;
+        c->raw_block = nullptr;
+        c->raw_bytes = 0;
+    }
+    bytes = align_up(bytes + bytes / 4, 1 << 20);
+    if (c->in_use + bytes > c->budget) return fail(DVM_ERR_OOM, "plugin scratch exceeds the HBM budget");
+    CK(cudaMalloc(&c->raw_block, bytes));
+    c->raw_bytes = bytes;
+    c->in_use += bytes;
+    return DVM_OK;
+}
+
+// Runs the batched self-induced kernel on caller buffers through table slot 0.
+static int raw_self(dvm_ctx* c, const double* x, const double* z, const double* circ,
+                    const double* sigma, uint64_t n, double* u, double* w, int precision,
+                    double kx0, double kz0, double kinv) {
+    if (n == 0) return DVM_OK;
+    if (n > 0xF0000000ull) return fail(DVM_ERR_ARG, "too many particles");
+    const uint64_t cap = align_up(n, kCapAlign);
+    InstDesc h;
+    std::memset(&h, 0, sizeof(h));
+    h.x = const_cast<double*>(x);
+    h.z = const_cast<double*>(z);
+    h.circ = const_cast<double*>(circ);
+    h.sigma = const_cast<double*>(sigma);
+    h.u = u;
+    h.w = w;
+    h.cap = (uint32_t)cap;
+    h.precision = precision;
+    h.kx0 = kx0;
+    h.kz0 = kz0;
+    h.kinv = kinv;
+    h.np = 1;
+    ListEntry e;
+    std::memset(&e, 0, sizeof(e));
+    e.inst = 0;
+    e.cap = (uint32_t)cap;
+    e.chunks = nbody_chunks(e.cap);
+    e.rhs_chunks = 1;
+    e.npad = 256;
+    int rc = ensure_workspace(c, cap, (uint64_t)e.chunks * cap, 256, 1, 1, false);
+    if (rc) return rc;
+    ListEntry* d_list = reinterpret_cast<ListEntry*>(c->ws.jobs);
+    InstState st0;
+    std::memset(&st0, 0, sizeof(st0));
+    st0.n = (uint32_t)n;
+    CK(cudaMemcpyAsync(c->d_table, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->d_state, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_list, &e, sizeof(e), cudaMemcpyHostToDevice, c->stream));
+    Workspace ws = c->ws;
+    ws.key_bits = key_bits_for(1);
+    ws.total_cap = cap;
+    biot_savart_self(c->d_table, c->d_state, d_list, 1, precision, ws, c->sms, c->stream);
+    g_launches += precision == kF32 ? 4 : 3;
+    CK(cudaGetLastError());
+    return DVM_OK;
+}
+
+int dvm_biot_savart_self_device(dvm_ctx* c, const double* x, const double* z, const double* circ,
+                                const double* sigma, uint64_t n, double* u, double* w,
+                                int precision) {
+    if (!c || (n && (!x || !z || !circ || !sigma || !u || !w))) return fail(DVM_ERR_ARG, "null argument");
+    if (precision != DVM_F64 && precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    return raw_self(c, x, z, circ, sigma, n, u, w, precision, -64.0, -64.0, 65536.0 / 128.0);
+}
+
+int dvm_biot_savart_self(dvm_ctx* c, const dvm_particle* p, uint64_t n, dvm_velocity* out,
+                         int precision) {
+    if (!c || (n && (!p || !out))) return fail(DVM_ERR_ARG, "null argument");
+    if (precision != DVM_F64 && precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
+    if (n == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    // AoS -> SoA on the host while computing the Morton domain.
+    std::vector<double> h(6 * n);
+    double xmn = p[0].x, xmx = p[0].x, zmn = p[0].z, zmx = p[0].z;
+    for (uint64_t i = 0; i < n; ++i) {
+        h[i] = p[i].x;
+        h[n + i] = p[i].z;
+        h[2 * n + i] = p[i].circ;
+        h[3 * n + i] = p[i].sigma;
+        xmn = std::min(xmn, p[i].x);
+        xmx = std::max(xmx, p[i].x);
+        zmn = std::min(zmn, p[i].z);
+        zmx = std::max(zmx, p[i].z);
+    }
+    int rc = raw_reserve(c, 8 * 6 * n);
+    if (rc) return rc;
+    double* d = static_cast<double*>(c->raw_block);
+    CK(cudaMemcpyAsync(d, h.data(), 8 * 4 * n, cudaMemcpyHostToDevice, c->stream));
+    double L = std::max(xmx - xmn, zmx - zmn);
+    if (!(L > 0)) L = 1.0;
+    rc = raw_self(c, d, d + n, d + 2 * n, d + 3 * n, n, d + 4 * n, d + 5 * n, precision, xmn, zmn,
+                  65535.0 / L);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(h.data() + 4 * n, d + 4 * n, 8 * 2 * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint64_t i = 0; i < n; ++i) {
+        out[i].u = h[4 * n + i];
+        out[i].w = h[5 * n + i];
+    }
+    return DVM_OK;
+}
+
+int dvm_biot_savart_at_device(dvm_ctx* c, const double* x, const double* z, const double* circ,
+                              const double* sigma, uint64_t ns, const double* tx, const double* tz,
+                              uint64_t nt, double* u, double* w, int precision, int skip_close) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    if (nt && (!tx || !tz || !u || !w)) return fail(DVM_ERR_ARG, "null target array");
+    if (ns && (!x || !z || !circ || !sigma)) return fail(DVM_ERR_ARG, "null source array");
+    if (precision != DVM_F64 && precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
+    if (nt == 0) return DVM_OK;
+    if (ns > 0xF0000000ull || nt > 0xF0000000ull) return fail(DVM_ERR_ARG, "too many points");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    const size_t elems = direct_at_part_elems((uint32_t)ns, (uint32_t)nt);
+    int rc = raw_reserve(c, 16 * elems);
+    if (rc) return rc;
+    direct_at_raw(x, z, circ, sigma, (uint32_t)ns, tx, tz, (uint32_t)nt, u, w, precision, skip_close,
+                  static_cast<double2*>(c->raw_block), c->sms, c->stream);
+    g_launches += 2;
+    CK(cudaGetLastError());
+    return DVM_OK;
+}
+
+int dvm_biot_savart_at(dvm_ctx* c, const dvm_particle* p, uint64_t ns, const double* tx,
+                       const double* tz, uint64_t nt, dvm_velocity* out, int precision) {
+    if (!c || (ns && !p) || (nt && (!tx || !tz || !out))) return fail(DVM_ERR_ARG, "null argument");
+    if (precision != DVM_F64 && precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
+    if (nt == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    const size_t elems = direct_at_part_elems((uint32_t)ns, (uint32_t)nt);
+    const size_t part_bytes = align_up(16 * elems, 256);
+    const size_t data_bytes = 8 * (4 * ns + 4 * nt);
+    int rc = raw_reserve(c, part_bytes + data_bytes);
+    if (rc) return rc;
+    char* base = static_cast<char*>(c->raw_block);
+    double* d = reinterpret_cast<double*>(base + part_bytes);
+    std::vector<double> h(4 * ns + 2 * nt);
+    for (uint64_t i = 0; i < ns; ++i) {
+        h[i] = p[i].x;
+        h[ns + i] = p[i].z;
+        h[2 * ns + i] = p[i].circ;
+        h[3 * ns + i] = p[i].sigma;
+    }
+    std::memcpy(h.data() + 4 * ns, tx, 8 * nt);
+    std::memcpy(h.data() + 4 * ns + nt, tz, 8 * nt);
+    CK(cudaMemcpyAsync(d, h.data(), 8 * h.size(), cudaMemcpyHostToDevice, c->stream));
+    double* du = d + 4 * ns + 2 * nt;
+    double* dw = du + nt;
+    direct_at_raw(d, d + ns, d + 2 * ns, d + 3 * ns, (uint32_t)ns, d + 4 * ns, d + 4 * ns + nt,
+                  (uint32_t)nt, du, dw, precision, 1, reinterpret_cast<double2*>(base), c->sms,
+                  c->stream);
+    g_launches += 2;
+    std::vector<double> r(2 * nt);
+    CK(cudaMemcpyAsync(r.data(), du, 8 * 2 * nt, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint64_t i = 0; i < nt; ++i) {
+        out[i].u = r[i];
+        out[i].w = r[nt + i];
+    }
+    return DVM_OK;
+}
+
+}  // extern "C"

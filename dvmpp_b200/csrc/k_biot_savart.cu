@@ -1,0 +1,704 @@
+// Regularised 2-D Biot-Savart kernels (reference: src/VelocityKernel.cpp:30-109,
+// src/VortexSheet.cpp:171-210).
+//
+// Pair kernel:  K(r2) = (1 - exp(-r2/sigma_j^2)) / r2   if r2 < 10 sigma_j^2
+//                     = 1 / r2                          otherwise
+//               u_i = -(1/2pi) sum_j K dz Gamma_j,  w_i = (1/2pi) sum_j K dx Gamma_j
+//
+// FP32 path (the throughput path): blobs of every listed simulation are sorted
+// along a Morton curve, packed as (x, z, Gamma, sigma) in FP64 and split into
+// 256-blob tiles with bounding boxes.  A work item is (simulation, 1024 sorted
+// targets, one source chunk); the persistent grid pulls items from an atomic
+// counter.  Each warp owns 128 consecutive sorted targets, so it covers a
+// small region: for every staged source tile it checks, once, whether any of
+// its pairs can fall inside the 10 sigma^2 core.  Far tiles (almost all of
+// them) run the 8-instruction pair loop with no test; near tiles run the exact
+// test, expm1 for the core and the self-pair exclusion.  Coordinates are FP32
+// offsets from the item's first target (which keeps close pairs accurate),
+// sums are plain FP32 within a 256-source stage and Kahan-compensated across
+// stages; chunk partials are combined in FP64 in chunk order (deterministic).
+//
+// FP64 path (the parity path): same work decomposition in original blob order
+// and the reference's exact operation sequence (no FMA contraction).
+#include <cfloat>
+#include <cub/cub.cuh>
+
+#include "dvm_device.cuh"
+#include "dvm_internal.h"
+
+namespace dvmk {
+namespace {
+
+constexpr int kMaxList = 1024;  // simulations per batched launch
+
+__device__ __forceinline__ uint32_t spread16(uint32_t v) {
+    v &= 0xFFFFu;
+    v = (v | (v << 8)) & 0x00FF00FFu;
+    v = (v | (v << 4)) & 0x0F0F0F0Fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t morton_key(double x, double z, double x0, double z0,
+                                               double inv) {
+    double fx = (x - x0) * inv, fz = (z - z0) * inv;
+    fx = fmin(fmax(fx, 0.0), 65535.0);
+    fz = fmin(fmax(fz, 0.0), 65535.0);
+    const uint32_t key = spread16((uint32_t)fx) | (spread16((uint32_t)fz) << 1);
+    return key == 0xFFFFFFFFu ? 0xFFFFFFFEu : key;
+}
+
+__device__ __forceinline__ int entry_of_slot(const ListEntry* list, int nlist, uint64_t g) {
+    int lo = 0, hi = nlist - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (list[mid].coff <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Sort keys over the concatenated capacity space: (entry << 32 | morton);
+// unused slots sort to the end of their simulation's range.
+__global__ void k_keys(const InstDesc* __restrict__ table, const InstState* __restrict__ st,
+                       const ListEntry* __restrict__ list, int nlist, uint64_t total,
+                       uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < total;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = entry_of_slot(list, nlist, g);
+        const ListEntry e = list[k];
+        const uint32_t i = (uint32_t)(g - e.coff);
+        const InstDesc& d = table[e.inst];
+        uint32_t mk = 0xFFFFFFFFu;
+        if (i < st[e.inst].n) mk = morton_key(d.x[i], d.z[i], d.kx0, d.kz0, d.kinv);
+        keys[g] = ((uint64_t)k << 32) | mk;
+        vals[g] = i;
+    }
+}
+
+// Gather (x, z, Gamma, sigma) into sorted order and record per-tile bounds.
+__global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ table,
+                                                const InstState* __restrict__ st,
+                                                const ListEntry* __restrict__ list, int nlist,
+                                                const uint32_t* __restrict__ perm,
+                                                double4* __restrict__ packed,
+                                                TileMeta* __restrict__ meta) {
+    __shared__ unsigned s_pre[kMaxList + 1];
+    __shared__ double s_red[5][kBsST / 32];
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += (st[list[k].inst].n + kBsST - 1) / kBsST;
+        }
+        s_pre[nlist] = acc;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[nlist];
+    for (unsigned item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const InstDesc& d = table[e.inst];
+        const uint32_t n = st[e.inst].n;
+        const uint32_t i = (item - s_pre[k]) * kBsST + threadIdx.x;
+        double xmin = DBL_MAX, xmax = -DBL_MAX, zmin = DBL_MAX, zmax = -DBL_MAX, thr = 0.0;
+        if (i < n) {
+            const uint32_t p = perm ? perm[e.coff + i] : i;
+            const double4 v = make_double4(d.x[p], d.z[p], d.circ[p], d.sigma[p]);
+            packed[e.coff + i] = v;
+            xmin = xmax = v.x;
+            zmin = zmax = v.y;
+            thr = 10.0 * (v.w * v.w);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            xmin = fmin(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+            xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+            zmin = fmin(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
+            zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
+            thr = fmax(thr, __shfl_xor_sync(0xffffffffu, thr, o));
+        }
+        const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            s_red[0][wid] = xmin;
+            s_red[1][wid] = xmax;
+            s_red[2][wid] = zmin;
+            s_red[3][wid] = zmax;
+            s_red[4][wid] = thr;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            TileMeta m;
+            m.xmin = s_red[0][0];
+            m.xmax = s_red[1][0];
+            m.zmin = s_red[2][0];
+            m.zmax = s_red[3][0];
+            m.thr = s_red[4][0];
+            for (int q = 1; q < kBsST / 32; ++q) {
+                m.xmin = fmin(m.xmin, s_red[0][q]);
+                m.xmax = fmax(m.xmax, s_red[1][q]);
+                m.zmin = fmin(m.zmin, s_red[2][q]);
+                m.zmax = fmax(m.zmax, s_red[3][q]);
+                m.thr = fmax(m.thr, s_red[4][q]);
+            }
+            m.pad0 = m.pad1 = m.pad2 = 0.0;
+            meta[(e.coff + (uint64_t)(item - s_pre[k]) * kBsST) / kBsST] = m;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void item_prefix_self(unsigned* s_pre, const InstState* st,
+                                                 const ListEntry* list, int nlist) {
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += ((st[list[k].inst].n + kBsTT - 1) / kBsTT) * (unsigned)list[k].chunks;
+        }
+        s_pre[nlist] = acc;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t chunk_size(uint32_t n, int chunks) {
+    uint32_t cs = (n + chunks - 1) / chunks;
+    return (cs + kBsST - 1) / kBsST * kBsST;
+}
+
+// ---- FP32 pair loops --------------------------------------------------------
+__device__ __forceinline__ void stage_far(const float4* __restrict__ src, const float (&tx)[kBsR],
+                                          const float (&tz)[kBsR], float (&pu)[kBsR],
+                                          float (&pw)[kBsR]) {
+#pragma unroll 8
+    for (int jj = 0; jj < kBsST; ++jj) {
+        const float4 s = src[jj];
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r) {
+            const float dx = tx[r] - s.x;
+            const float dz = tz[r] - s.y;
+            const float r2 = fmaf(dx, dx, dz * dz);
+            const float g = rcp_approx(r2) * s.z;
+            pu[r] = fmaf(-g, dz, pu[r]);
+            pw[r] = fmaf(g, dx, pw[r]);
+        }
+    }
+}
+
+__device__ __forceinline__ void stage_near(const float4* __restrict__ src,
+                                           const float* __restrict__ rs,
+                                           const float (&tx)[kBsR], const float (&tz)[kBsR],
+                                           float (&pu)[kBsR], float (&pw)[kBsR], int tbase,
+                                           int jbase) {
+#pragma unroll 2
+    for (int jj = 0; jj < kBsST; ++jj) {
+        const float4 s = src[jj];
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r) {
+            const float dx = tx[r] - s.x;
+            const float dz = tz[r] - s.y;
+            const float r2 = fmaf(dx, dx, dz * dz);
+            float K = rcp_approx(r2);
+            if (r2 < s.w) {
+                // 1 - exp(-r2/sigma^2) through expm1 keeps close pairs accurate.
+                const float e = expm1f(-r2 * rs[jj]);
+                K = (tbase + r == jbase + jj) ? 0.0f : -e * K;
+            }
+            const float g = K * s.z;
+            pu[r] = fmaf(-g, dz, pu[r]);
+            pw[r] = fmaf(g, dx, pw[r]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBsThreads, 2)
+    k_self_f32(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
+               const double4* __restrict__ packed, const TileMeta* __restrict__ meta,
+               double2* __restrict__ part, unsigned* __restrict__ work) {
+    __shared__ unsigned s_pre[kMaxList + 1];
+    __shared__ float4 s_src[kBsST];
+    __shared__ float s_rs[kBsST];
+    __shared__ unsigned s_item;
+    item_prefix_self(s_pre, st, list, nlist);
+    const unsigned total = s_pre[nlist];
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(work, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const uint32_t n = st[e.inst].n;
+        const unsigned local = item - s_pre[k];
+        const uint32_t tile = local / e.chunks, c = local % e.chunks;
+        const uint32_t t0 = tile * kBsTT;
+        const uint32_t cs = chunk_size(n, e.chunks);
+        const uint32_t j0 = c * cs, j1 = min(n, j0 + cs);
+        const double4* __restrict__ P = packed + e.coff;
+        const double ox = P[t0].x, oz = P[t0].y;
+
+        float tx[kBsR], tz[kBsR];
+        double wxmin = DBL_MAX, wxmax = -DBL_MAX, wzmin = DBL_MAX, wzmax = -DBL_MAX;
+        const uint32_t tb = t0 + tid * kBsR;
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r) {
+            tx[r] = 0.0f;
+            tz[r] = 0.0f;
+            if (tb + r < n) {
+                const double4 p = P[tb + r];
+                tx[r] = (float)(p.x - ox);
+                tz[r] = (float)(p.y - oz);
+                wxmin = fmin(wxmin, p.x);
+                wxmax = fmax(wxmax, p.x);
+                wzmin = fmin(wzmin, p.y);
+                wzmax = fmax(wzmax, p.y);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            wxmin = fmin(wxmin, __shfl_xor_sync(0xffffffffu, wxmin, o));
+            wxmax = fmax(wxmax, __shfl_xor_sync(0xffffffffu, wxmax, o));
+            wzmin = fmin(wzmin, __shfl_xor_sync(0xffffffffu, wzmin, o));
+            wzmax = fmax(wzmax, __shfl_xor_sync(0xffffffffu, wzmax, o));
+        }
+        float su[kBsR], cu[kBsR], sw[kBsR], cw[kBsR];
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
+
+        for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
+            __syncthreads();
+            const uint32_t j = s0 + tid;
+            if (j < j1) {
+                const double4 p = P[j];
+                const double s2 = p.w * p.w;
+                s_src[tid] = make_float4((float)(p.x - ox), (float)(p.y - oz), (float)p.z,
+                                         (float)(10.0 * s2));
+                s_rs[tid] = (float)(1.0 / s2);
+            } else {
+                s_src[tid] = make_float4(1e18f, 1e18f, 0.0f, -1.0f);
+                s_rs[tid] = 0.0f;
+            }
+            __syncthreads();
+            const TileMeta m = meta[(e.coff + s0) / kBsST];
+            const double gx = fmax(0.0, fmax(m.xmin - wxmax, wxmin - m.xmax));
+            const double gz = fmax(0.0, fmax(m.zmin - wzmax, wzmin - m.zmax));
+            float pu[kBsR], pw[kBsR];
+#pragma unroll
+            for (int r = 0; r < kBsR; ++r) pu[r] = pw[r] = 0.0f;
+            if (gx * gx + gz * gz > m.thr * 1.001 + 1e-30) {
+                stage_far(s_src, tx, tz, pu, pw);
+            } else {
+                stage_near(s_src, s_rs, tx, tz, pu, pw, (int)tb, (int)s0);
+            }
+#pragma unroll
+            for (int r = 0; r < kBsR; ++r) {  // Kahan fold of the stage partial
+                float y = pu[r] - cu[r];
+                float t = su[r] + y;
+                cu[r] = (t - su[r]) - y;
+                su[r] = t;
+                y = pw[r] - cw[r];
+                t = sw[r] + y;
+                cw[r] = (t - sw[r]) - y;
+                sw[r] = t;
+            }
+        }
+        double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r)
+            if (tb + r < n)
+                out[tb + r] = make_double2((double)su[r] - (double)cu[r],
+                                           (double)sw[r] - (double)cw[r]);
+    }
+}
+
+// ---- FP64, reference operation order ---------------------------------------
+__global__ void __launch_bounds__(kBsThreads, 1)
+    k_self_f64(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
+               const double4* __restrict__ packed, double2* __restrict__ part,
+               unsigned* __restrict__ work) {
+    __shared__ unsigned s_pre[kMaxList + 1];
+    __shared__ double4 s_src[kBsST];  // x, z, circ, threshold
+    __shared__ double s_rs[kBsST];
+    __shared__ unsigned s_item;
+    item_prefix_self(s_pre, st, list, nlist);
+    const unsigned total = s_pre[nlist];
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(work, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const uint32_t n = st[e.inst].n;
+        const unsigned local = item - s_pre[k];
+        const uint32_t tile = local / e.chunks, c = local % e.chunks;
+        const uint32_t cs = chunk_size(n, e.chunks);
+        const uint32_t j0 = c * cs, j1 = min(n, j0 + cs);
+        const double4* __restrict__ P = packed + e.coff;
+        const uint32_t tb = tile * kBsTT + tid * kBsR;
+        double tx[kBsR], tz[kBsR], uu[kBsR], ww[kBsR];
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r) {
+            const double4 p = (tb + r < n) ? P[tb + r] : make_double4(0, 0, 0, 1);
+            tx[r] = p.x;
+            tz[r] = p.y;
+            uu[r] = ww[r] = 0.0;
+        }
+        for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
+            __syncthreads();
+            const uint32_t j = s0 + tid;
+            if (j < j1) {
+                const double4 p = P[j];
+                const double s2 = dmul(p.w, p.w);
+                s_src[tid] = make_double4(p.x, p.y, p.z, dmul(10.0, s2));
+                s_rs[tid] = ddiv(1.0, s2);
+            }
+            __syncthreads();
+            const int cnt = (int)min((uint32_t)kBsST, j1 - s0);
+            for (int jj = 0; jj < cnt; ++jj) {
+                const double4 s = s_src[jj];
+#pragma unroll
+                for (int r = 0; r < kBsR; ++r) {
+                    if (tb + r == s0 + jj) continue;  // i != j (src/VelocityKernel.cpp:43)
+                    const double dx = dsub(tx[r], s.x);
+                    const double dz = dsub(tz[r], s.y);
+                    const double r2 = dadd(dmul(dx, dx), dmul(dz, dz));
+                    double K;
+                    if (r2 < s.w) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
+                    else K = ddiv(1.0, r2);
+                    uu[r] = dsub(uu[r], dmul(dmul(K, dz), s.z));
+                    ww[r] = dadd(ww[r], dmul(dmul(K, dx), s.z));
+                }
+            }
+        }
+        double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
+#pragma unroll
+        for (int r = 0; r < kBsR; ++r)
+            if (tb + r < n) out[tb + r] = make_double2(uu[r], ww[r]);
+    }
+}
+
+// Sum chunk partials in chunk order, scale by 1/(2 pi), scatter to blob order.
+__global__ void k_self_combine(const InstDesc* __restrict__ table,
+                               const InstState* __restrict__ st,
+                               const ListEntry* __restrict__ list, int nlist,
+                               const uint32_t* __restrict__ perm,
+                               const double2* __restrict__ part) {
+    __shared__ unsigned s_pre[kMaxList + 1];
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += (st[list[k].inst].n + blockDim.x - 1) / blockDim.x;
+        }
+        s_pre[nlist] = acc;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[nlist];
+    for (unsigned item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const uint32_t n = st[e.inst].n;
+        const uint32_t t = (item - s_pre[k]) * blockDim.x + threadIdx.x;
+        if (t >= n) continue;
+        double su = 0.0, sw = 0.0;
+        for (int c = 0; c < e.chunks; ++c) {
+            const double2 v = part[e.poff + (uint64_t)c * e.cap + t];
+            su += v.x;
+            sw += v.y;
+        }
+        const InstDesc& d = table[e.inst];
+        const uint32_t p = perm ? perm[e.coff + t] : t;
+        d.u[p] = su * kRpi2;
+        d.w[p] = sw * kRpi2;
+    }
+}
+
+// ---- arbitrary targets --------------------------------------------------------
+// One item = (entry, 256 targets, kAtChunk sources).  Sources are staged with
+// FP64 positions; each pair forms dx, dz in FP64 (exact for close pairs) and,
+// in FP32 mode, evaluates the kernel in FP32 with a Kahan fold per stage.
+struct AtJob {
+    const double* tx;
+    const double* tz;
+    uint32_t nt;
+    int skip_close;  // 1: pairs with r2 <= 1e-15 skipped (computeInducedAt)
+    const double* sx;
+    const double* sz;
+    const double* sc;
+    const double* ss;
+    const uint32_t* pns;  // source count on the device, or null -> ns
+    uint32_t ns;
+    int npad;             // partial row length
+    double2* part;        // [chunk][npad]
+    double* circ_part;    // [chunk], or null
+};
+
+template <bool F32>
+__global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int njobs) {
+    __shared__ unsigned s_pre[kMaxList + 1];
+    __shared__ double s_x[256], s_z[256], s_c[256], s_thr[256], s_rs[256];
+    __shared__ double s_red[8];
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < njobs; ++k) {
+            s_pre[k] = acc;
+            const uint32_t ns = jobs[k].pns ? *jobs[k].pns : jobs[k].ns;
+            acc += ((jobs[k].nt + 255) / 256) * ((ns + kAtChunk - 1) / kAtChunk);
+        }
+        s_pre[njobs] = acc;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[njobs];
+    for (unsigned item = blockIdx.x; item < total; item += gridDim.x) {
+        const int k = locate(s_pre, njobs, item);
+        const AtJob J = jobs[k];
+        const uint32_t ns = J.pns ? *J.pns : J.ns;
+        const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+        const unsigned local = item - s_pre[k];
+        const uint32_t ttile = local / nchunk, c = local % nchunk;
+        const uint32_t t = ttile * 256 + threadIdx.x;
+        const double tx = t < J.nt ? J.tx[t] : 0.0, tz = t < J.nt ? J.tz[t] : 0.0;
+        const uint32_t j0 = c * kAtChunk, j1 = min(ns, j0 + kAtChunk);
+        double uu = 0.0, ww = 0.0, csum = 0.0;
+        float su = 0.f, cu = 0.f, sw = 0.f, cw = 0.f;
+        for (uint32_t s0 = j0; s0 < j1; s0 += 256) {
+            __syncthreads();
+            const uint32_t j = s0 + threadIdx.x;
+            if (j < j1) {
+                const double sg = J.ss[j];
+                const double s2 = dmul(sg, sg);
+                s_x[threadIdx.x] = J.sx[j];
+                s_z[threadIdx.x] = J.sz[j];
+                s_c[threadIdx.x] = J.sc[j];
+                s_thr[threadIdx.x] = dmul(10.0, s2);
+                s_rs[threadIdx.x] = ddiv(1.0, s2);
+                if (ttile == 0) csum += J.sc[j];
+            }
+            __syncthreads();
+            const int cnt = (int)min(256u, j1 - s0);
+            if (F32) {
+                float pu = 0.f, pw = 0.f;
+                for (int jj = 0; jj < cnt; ++jj) {
+                    const float dx = (float)(tx - s_x[jj]);
+                    const float dz = (float)(tz - s_z[jj]);
+                    const float r2 = fmaf(dx, dx, dz * dz);
+                    if (J.skip_close && !(r2 > 1e-15f)) continue;
+                    float K = rcp_approx(r2);
+                    if (r2 < (float)s_thr[jj]) K = -expm1f(-r2 * (float)s_rs[jj]) * K;
+                    const float g = K * (float)s_c[jj];
+                    pu = fmaf(-g, dz, pu);
+                    pw = fmaf(g, dx, pw);
+                }
+                float y = pu - cu, tt = su + y;
+                cu = (tt - su) - y;
+                su = tt;
+                y = pw - cw;
+                tt = sw + y;
+                cw = (tt - sw) - y;
+                sw = tt;
+            } else {
+                for (int jj = 0; jj < cnt; ++jj) {
+                    const double dx = dsub(tx, s_x[jj]);
+                    const double dz = dsub(tz, s_z[jj]);
+                    const double r2 = dadd(dmul(dx, dx), dmul(dz, dz));
+                    if (J.skip_close && !(r2 > 1e-15)) continue;
+                    double K;
+                    if (r2 < s_thr[jj]) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
+                    else K = ddiv(1.0, r2);
+                    uu = dsub(uu, dmul(dmul(K, dz), s_c[jj]));
+                    ww = dadd(ww, dmul(dmul(K, dx), s_c[jj]));
+                }
+            }
+        }
+        if (F32) {
+            uu = (double)su - (double)cu;
+            ww = (double)sw - (double)cw;
+        }
+        if (t < J.nt) J.part[(uint64_t)c * J.npad + t] = make_double2(uu, ww);
+        if (ttile == 0 && J.circ_part) {
+            for (int o = 16; o > 0; o >>= 1) csum += __shfl_xor_sync(0xffffffffu, csum, o);
+            if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = csum;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double a = 0.0;
+                for (int q = 0; q < 8; ++q) a += s_red[q];
+                J.circ_part[c] = a;
+            }
+        }
+    }
+}
+
+__global__ void k_at_combine(const AtJob* __restrict__ jobs, double* __restrict__ u,
+                             double* __restrict__ w) {
+    const AtJob J = jobs[0];
+    const uint32_t ns = J.pns ? *J.pns : J.ns;
+    const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < J.nt; t += gridDim.x * blockDim.x) {
+        double su = 0.0, sw = 0.0;
+        for (uint32_t c = 0; c < nchunk; ++c) {
+            const double2 v = J.part[(uint64_t)c * J.npad + t];
+            su += v.x;
+            sw += v.y;
+        }
+        u[t] = su * kRpi2;
+        w[t] = sw * kRpi2;
+    }
+}
+
+// b_i = (Ux + u_i) enx_i + (Uz + w_i) enz_i, b_np = -sum(circ)
+// (src/VortexSheet.cpp:206-210); one block per simulation.
+__global__ void k_rhs_combine(const InstDesc* __restrict__ table, InstState* __restrict__ st,
+                              const ListEntry* __restrict__ list, const AtJob* __restrict__ jobs) {
+    const int k = blockIdx.x;
+    const ListEntry e = list[k];
+    const InstDesc& d = table[e.inst];
+    const AtJob J = jobs[k];
+    const uint32_t ns = st[e.inst].n;
+    const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    for (int i = threadIdx.x; i < d.np; i += blockDim.x) {
+        double su = 0.0, sw = 0.0;
+        for (uint32_t c = 0; c < nchunk; ++c) {
+            const double2 v = J.part[(uint64_t)c * J.npad + i];
+            su += v.x;
+            sw += v.y;
+        }
+        const double ui = dmul(su, kRpi2), wi = dmul(sw, kRpi2);
+        d.b[i] = dadd(dmul(dadd(d.ux, ui), d.enx[i]), dmul(dadd(d.uz, wi), d.enz[i]));
+    }
+    if (threadIdx.x == 0) {
+        double tc = 0.0;
+        for (uint32_t c = 0; c < nchunk; ++c) tc += J.circ_part[c];
+        d.b[d.np] = -tc;
+        st[e.inst].totalcirc = tc;
+    }
+}
+
+__global__ void k_build_rhs_jobs(const InstDesc* __restrict__ table, InstState* __restrict__ st,
+                                 const ListEntry* __restrict__ list, int nlist,
+                                 double2* rhs_part, double* circ_part, AtJob* jobs) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlist) return;
+    const ListEntry e = list[k];
+    const InstDesc& d = table[e.inst];
+    AtJob J;
+    J.tx = d.xc;
+    J.tz = d.zc;
+    J.nt = (uint32_t)d.np;
+    J.skip_close = 0;  // solvevortexsheet has no close-pair skip (src/VortexSheet.cpp:186-203)
+    J.sx = d.x;
+    J.sz = d.z;
+    J.sc = d.circ;
+    J.ss = d.sigma;
+    J.pns = &st[e.inst].n;
+    J.ns = 0;
+    J.npad = e.npad;
+    J.part = rhs_part + e.roff;
+    J.circ_part = circ_part + e.cofs;
+    jobs[k] = J;
+}
+
+}  // namespace
+
+size_t cub_sort_bytes(uint64_t total) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                    (const uint32_t*)nullptr, (uint32_t*)nullptr, (int64_t)total,
+                                    0, 48);
+    return bytes;
+}
+
+void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                         int precision, const Workspace& ws, int sms, cudaStream_t s) {
+    const uint32_t* perm = nullptr;
+    if (precision == kF32) {
+        const int g = (int)std::min<uint64_t>((ws.total_cap + 255) / 256, (uint64_t)sms * 16);
+        k_keys<<<g, 256, 0, s>>>(table, st, list, nlist, ws.total_cap, ws.keys_in, ws.vals_in);
+        size_t bytes = ws.cub_bytes;
+        cub::DeviceRadixSort::SortPairs(ws.cub_tmp, bytes, ws.keys_in, ws.keys_out, ws.vals_in,
+                                        ws.perm, (int64_t)ws.total_cap, 0, ws.key_bits, s);
+        perm = ws.perm;
+    }
+    k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, ws.meta);
+    cudaMemsetAsync(ws.work, 0, sizeof(unsigned), s);
+}
+
+void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                         int precision, const Workspace& ws, int sms, cudaStream_t s) {
+    (void)table;
+    if (precision == kF32)
+        k_self_f32<<<sms * 2, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.meta, ws.part,
+                                                  ws.work);
+    else
+        k_self_f64<<<sms, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part, ws.work);
+}
+
+void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                        int precision, const Workspace& ws, int sms, cudaStream_t s) {
+    k_self_combine<<<sms * 8, 256, 0, s>>>(table, st, list, nlist,
+                                           precision == kF32 ? ws.perm : nullptr, ws.part);
+}
+
+void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                      int precision, const Workspace& ws, int sms, cudaStream_t s) {
+    biot_savart_prepare(table, st, list, nlist, precision, ws, sms, s);
+    biot_savart_compute(table, st, list, nlist, precision, ws, sms, s);
+    biot_savart_finish(table, st, list, nlist, precision, ws, sms, s);
+}
+
+void sheet_rhs(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+               int precision, const Workspace& ws, int sms, cudaStream_t s) {
+    static_assert(sizeof(AtJob) <= 256, "job record size");
+    AtJob* jobs = reinterpret_cast<AtJob*>(ws.jobs);
+    k_build_rhs_jobs<<<(nlist + 127) / 128, 128, 0, s>>>(table, st, list, nlist, ws.rhs_part,
+                                                         ws.circ_part, jobs);
+    if (precision == kF32) k_at<true><<<sms * 4, 256, 0, s>>>(jobs, nlist);
+    else k_at<false><<<sms * 4, 256, 0, s>>>(jobs, nlist);
+    k_rhs_combine<<<nlist, 256, 0, s>>>(table, st, list, jobs);
+}
+
+size_t direct_at_part_elems(uint32_t ns, uint32_t nt) {
+    const size_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    const size_t npad = (nt + 255) / 256 * 256;
+    return std::max<size_t>(1, nchunk) * std::max<size_t>(npad, 256) + 64;
+}
+
+void direct_at_raw(const double* x, const double* z, const double* circ, const double* sigma,
+                   uint32_t ns, const double* tx, const double* tz, uint32_t nt, double* u,
+                   double* w, int precision, int skip_close, double2* part, int sms,
+                   cudaStream_t s) {
+    // The job record sits in the last 64 entries of the partials buffer.
+    const size_t elems = direct_at_part_elems(ns, nt);
+    AtJob* job = reinterpret_cast<AtJob*>(part + elems - 64);
+    AtJob J;
+    J.tx = tx;
+    J.tz = tz;
+    J.nt = nt;
+    J.skip_close = skip_close;
+    J.sx = x;
+    J.sz = z;
+    J.sc = circ;
+    J.ss = sigma;
+    J.pns = nullptr;
+    J.ns = ns;
+    J.npad = (int)std::max<size_t>((nt + 255) / 256 * 256, 256);
+    J.part = part;
+    J.circ_part = nullptr;
+    cudaMemcpyAsync(job, &J, sizeof(AtJob), cudaMemcpyHostToDevice, s);
+    if (ns > 0) {
+        if (precision == kF32) k_at<true><<<sms * 4, 256, 0, s>>>(job, 1);
+        else k_at<false><<<sms * 4, 256, 0, s>>>(job, 1);
+        k_at_combine<<<std::max<uint32_t>(1, std::min<uint32_t>((nt + 255) / 256, sms * 8)), 256, 0,
+                       s>>>(job, u, w);
+    } else {
+        cudaMemsetAsync(u, 0, sizeof(double) * nt, s);
+        cudaMemsetAsync(w, 0, sizeof(double) * nt, s);
+    }
+}
+
+}  // namespace dvmk

@@ -1,0 +1,460 @@
+// Bookkeeping kernels of the step: random-walk diffusion
+// (src/VortexBlobs.cpp:251-265), nascent-vortex release + append
+// (src/VortexSheet.cpp:275-333, src/VortexBlobs.cpp:211-227) and surface
+// crossing (src/VortexSheet.cpp:345-464, dispatch src/DVMBase.cpp:107-118).
+//
+// These are HBM-bound integer/byte work around FP64 positions.  Counts are
+// exact: release counts come from the same FP64 arithmetic as the reference,
+// the inside test is the reference's crossing-number test with one rounding
+// per operation, and DELETE is a stable (order-preserving) compaction.
+#include <cfloat>
+
+#include "dvm_device.cuh"
+#include "dvm_internal.h"
+
+namespace dvmk {
+namespace {
+
+__device__ __forceinline__ void raise_status(InstState& s, int code) {
+    atomicCAS(&s.status, 0, code);
+}
+
+// ---- diffusion -------------------------------------------------------------------
+__global__ void k_diffuse(const InstDesc* __restrict__ table, InstState* __restrict__ st,
+                          const ListEntry* __restrict__ list, int nlist) {
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    InstState& S = st[e.inst];
+    if (S.status) return;
+    const uint32_t n = S.n;
+    const uint64_t cur = S.cursor;
+    if (d.rng == kInject && cur + 2ull * n > d.ucount) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(S, kErrRngExhausted);
+        return;
+    }
+    const double c4 = dmul(dmul(4.0, d.nu), d.dt);
+    const double twopi = dmul(2.0, kPi);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double R1, R2;
+        if (d.rng == kInject) {
+            R1 = d.uniforms[cur + 2ull * i];
+            R2 = d.uniforms[cur + 2ull * i + 1];
+        } else {
+            philox_uniform2(d.seed, i, S.step, d.uid, 0u, R1, R2);
+        }
+        const double rrw = sqrt(dmul(c4, log(ddiv(1.0, R1))));
+        const double th = dmul(twopi, R2);
+        d.x[i] = dadd(d.x[i], dmul(rrw, cos(th)));
+        d.z[i] = dadd(d.z[i], dmul(rrw, sin(th)));
+    }
+}
+
+// ---- release + append: one block per simulation -------------------------------------
+constexpr int kRelThreads = 256;
+
+__global__ void __launch_bounds__(kRelThreads) k_release(const InstDesc* __restrict__ table,
+                                                         InstState* __restrict__ st,
+                                                         const ListEntry* __restrict__ list) {
+    extern __shared__ double s_dyn[];  // counts[np] | circ_new[np]
+    __shared__ double s_red[kRelThreads / 32];
+    __shared__ uint32_t s_part[kRelThreads + 1];
+    __shared__ int s_bad;
+    const ListEntry e = list[blockIdx.x];
+    const InstDesc& d = table[e.inst];
+    InstState& S = st[e.inst];
+    if (S.status) return;
+    const int np = d.np;
+    double* cnt = s_dyn;
+    double* cnew = s_dyn + np;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_bad = 0;
+    // Signed maximum of the panel circulations (src/VortexSheet.cpp:282-285).
+    double mx = -DBL_MAX;
+    for (int j = tid; j < np; j += kRelThreads) mx = fmax(mx, dmul(d.gamma[j], d.ds[j]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((tid & 31) == 0) s_red[tid >> 5] = mx;
+    __syncthreads();
+    mx = s_red[0];
+    for (int q = 1; q < kRelThreads / 32; ++q) mx = fmax(mx, s_red[q]);
+    // Arma's max: NaN elements never replace the running maximum; fmax skips
+    // NaN the same way, and a NaN in any count is caught below as in :289.
+    const double Md = (double)d.M;
+    // Contiguous panel ranges per thread so the scan below is in panel order.
+    const int per = (np + kRelThreads - 1) / kRelThreads;
+    const int jb = tid * per, je = min(np, jb + per);
+    uint32_t mine = 0;
+    for (int j = jb; j < je; ++j) {
+        const double pc = dmul(d.gamma[j], d.ds[j]);
+        const double c = dadd(floor(fabs(dmul(ddiv(pc, mx), Md))), 1.0);
+        cnt[j] = c;
+        cnew[j] = ddiv(pc, c);
+        if (!(c > 1.0e-15)) s_bad = 1;
+        else mine += (uint32_t)c;
+    }
+    s_part[tid] = mine;
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t acc = 0;
+        for (int t = 0; t < kRelThreads; ++t) {
+            const uint32_t v = s_part[t];
+            s_part[t] = acc;
+            acc += v;
+        }
+        s_part[kRelThreads] = acc;
+    }
+    __syncthreads();
+    if (s_bad) {  // the reference throws VortexException (src/VortexSheet.cpp:289-291)
+        if (tid == 0) raise_status(S, kErrRelease);
+        return;
+    }
+    const uint32_t n0 = S.n;
+    const uint32_t nrv = s_part[kRelThreads];
+    const uint64_t cur = S.cursor;
+    if ((uint64_t)n0 + nrv > d.cap) {
+        if (tid == 0) raise_status(S, kErrCapacity);
+        return;
+    }
+    if (d.rng == kInject && cur + 2ull * n0 + nrv > d.ucount) {
+        if (tid == 0) raise_status(S, kErrRngExhausted);
+        return;
+    }
+    const double c4 = dmul(dmul(4.0, d.nu), d.dt);
+    uint32_t o = n0 + s_part[tid];
+    for (int j = jb; j < je; ++j) {
+        const uint32_t c = (uint32_t)cnt[j];
+        const double xm = dadd(d.xp[j], ddiv(dmul(d.ds[j], d.etx[j]), dadd(cnt[j], 1.0)));
+        const double zm = dadd(d.zp[j], ddiv(dmul(d.ds[j], d.etz[j]), dadd(cnt[j], 1.0)));
+        for (uint32_t q = 0; q < c; ++q, ++o) {
+            const uint32_t r = o - n0;  // release index, panel order
+            double R;
+            if (d.rng == kInject) {
+                R = d.uniforms[cur + 2ull * n0 + r];
+            } else {
+                double R2;
+                philox_uniform2(d.seed, r, S.step, d.uid, 1u, R, R2);
+            }
+            const double rrw = fabs(sqrt(dmul(c4, log(ddiv(1.0, R)))));
+            d.x[o] = dadd(xm, dmul(rrw, d.enx[j]));
+            d.z[o] = dadd(zm, dmul(rrw, d.enz[j]));
+            d.circ[o] = cnew[j];
+            d.sigma[o] = d.psigma[j];
+            d.u[o] = 0.0;
+            d.w[o] = 0.0;
+            d.uvs[o] = 0.0;
+            d.wvs[o] = 0.0;
+            d.id[o] = n0;  // nascent IDs are 0, shifted by Nold (src/VortexBlobs.cpp:215-217)
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        S.n = n0 + nrv;
+        if (d.rng == kInject) S.cursor = cur + 2ull * n0 + nrv;
+    }
+}
+
+// ---- crossing test ----------------------------------------------------------------
+struct Body {
+    const double* xp;
+    const double* zp;
+    int np;
+};
+
+// Crossing-number test, cn == 1 (src/VortexSheet.cpp:447-464).  Points outside
+// the contour's z-range, or to the right of its padded x-range, cross no edge.
+__device__ __forceinline__ bool inside_body(const double* __restrict__ xp,
+                                            const double* __restrict__ zp, int np, double xc,
+                                            double zc, double bxmax, double bzmin, double bzmax) {
+    if (zc < bzmin || zc >= bzmax || xc > bxmax) return false;
+    int cn = 0;
+    for (int i = 0; i < np; ++i) {
+        const double z0 = zp[i], z1 = zp[i + 1];
+        if (((z0 <= zc) && (z1 > zc)) || ((z0 > zc) && (z1 <= zc))) {
+            const double vt = ddiv(dsub(zc, z0), dsub(z1, z0));
+            if (xc < dadd(xp[i], dmul(vt, dsub(xp[i + 1], xp[i])))) ++cn;
+        }
+    }
+    return cn == 1;
+}
+
+__device__ __forceinline__ void load_contour(const InstDesc& d, double* sx, double* sz,
+                                             double* snx, double* snz) {
+    for (int j = threadIdx.x; j <= d.np; j += blockDim.x) {
+        sx[j] = d.xp[j];
+        sz[j] = d.zp[j];
+        if (j < d.np) {
+            snx[j] = d.enx[j];
+            snz[j] = d.enz[j];
+        }
+    }
+}
+
+// REFLECT / ABSORB (src/VortexSheet.cpp:345-405): each blob moves independently.
+__global__ void __launch_bounds__(256) k_reflect(const InstDesc* __restrict__ table,
+                                                 const InstState* __restrict__ st,
+                                                 const ListEntry* __restrict__ list, int nlist,
+                                                 unsigned* __restrict__ work) {
+    extern __shared__ double s_c[];
+    __shared__ unsigned s_pre[1025];
+    __shared__ unsigned s_item;
+    __shared__ int s_loaded;
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += st[list[k].inst].status ? 0u : (st[list[k].inst].n + 255) / 256;
+        }
+        s_pre[nlist] = acc;
+        s_loaded = -1;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[nlist];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(work, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= total) break;
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const InstDesc& d = table[e.inst];
+        const int np = d.np;
+        double* sx = s_c;
+        double* sz = sx + (np + 1);
+        double* snx = sz + (np + 1);
+        double* snz = snx + np;
+        if (s_loaded != k) load_contour(d, sx, sz, snx, snz);
+        __syncthreads();
+        if (threadIdx.x == 0) s_loaded = k;
+        const uint32_t n = st[e.inst].n;
+        const uint32_t i = (item - s_pre[k]) * 256 + threadIdx.x;
+        if (i < n) {
+            const double px = d.x[i], pz = d.z[i];
+            if (inside_body(sx, sz, np, px, pz, d.bxmax, d.bzmin, d.bzmax)) {
+                int cp = 0;
+                double md = 1e10;
+                for (int j = 0; j < np; ++j) {
+                    const double x0 = sx[j], z0 = sz[j], x1 = sx[j + 1], z1 = sz[j + 1];
+                    const double vx = dsub(px, x0), vz = dsub(pz, z0);
+                    const double dx = dsub(x1, x0), dz = dsub(z1, z0);
+                    const double len = dadd(dmul(dx, dx), dmul(dz, dz));
+                    double t = ddiv(dadd(dmul(vx, dx), dmul(vz, dz)), len);
+                    t = (t < 1.0) ? t : 1.0;  // std::min(1.0, t)
+                    t = (0.0 < t) ? t : 0.0;  // std::max(0.0, .)
+                    const double cx = dadd(x0, dmul(t, dx)), cz = dadd(z0, dmul(t, dz));
+                    const double ex = dsub(px, cx), ez = dsub(pz, cz);
+                    const double dist = sqrt(dadd(dmul(ex, ex), dmul(ez, ez)));
+                    if (dist < md) {
+                        md = dist;
+                        cp = j;
+                    }
+                }
+                const double off = dadd(dmul(2.0, md), 1e-6);
+                double nx = dadd(px, dmul(off, snx[cp]));
+                double nz = dadd(pz, dmul(off, snz[cp]));
+                if (inside_body(sx, sz, np, nx, nz, d.bxmax, d.bzmin, d.bzmax)) {
+                    nx = dadd(px, dmul(dmul(3.0, off), snx[cp]));
+                    nz = dadd(pz, dmul(dmul(3.0, off), snz[cp]));
+                }
+                d.x[i] = nx;
+                d.z[i] = nz;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// DELETE (src/VortexSheet.cpp:407-445): keep flags and kept count per 1024-tile.
+constexpr int kDelTile = 1024;
+
+__global__ void __launch_bounds__(256) k_del_flags(const InstDesc* __restrict__ table,
+                                                   const InstState* __restrict__ st,
+                                                   const ListEntry* __restrict__ list,
+                                                   uint8_t* __restrict__ flags,
+                                                   uint32_t* __restrict__ tile_counts) {
+    extern __shared__ double s_c[];
+    __shared__ uint32_t s_cnt;
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const InstState& S = st[e.inst];
+    const uint32_t n = S.n;
+    const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
+    if (S.status) return;
+    double* sx = s_c;
+    double* sz = sx + (d.np + 1);
+    double* snx = sz + (d.np + 1);
+    double* snz = snx + d.np;
+    load_contour(d, sx, sz, snx, snz);
+    __syncthreads();
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (threadIdx.x == 0) s_cnt = 0;
+        __syncthreads();
+        uint32_t mine = 0;
+        for (uint32_t q = threadIdx.x; q < kDelTile; q += blockDim.x) {
+            const uint32_t i = t * kDelTile + q;
+            if (i >= n) break;
+            const uint8_t keep =
+                inside_body(sx, sz, d.np, d.x[i], d.z[i], d.bxmax, d.bzmin, d.bzmax) ? 0 : 1;
+            flags[e.coff + i] = keep;
+            mine += keep;
+        }
+        for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, mine);
+        __syncthreads();
+        if (threadIdx.x == 0) tile_counts[e.coff / kDelTile + t] = s_cnt;
+        __syncthreads();
+    }
+}
+
+// Stable scatter of kept blobs into the staging area (8 FP64 arrays + ids).
+__global__ void __launch_bounds__(kDelTile) k_del_compact(const InstDesc* __restrict__ table,
+                                                          const InstState* __restrict__ st,
+                                                          const ListEntry* __restrict__ list,
+                                                          const uint8_t* __restrict__ flags,
+                                                          const uint32_t* __restrict__ tile_counts,
+                                                          double* __restrict__ stage,
+                                                          uint64_t total_cap) {
+    __shared__ uint32_t s_warp[kDelTile / 32];
+    __shared__ uint32_t s_base, s_kept;
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const InstState& S = st[e.inst];
+    if (S.status) return;
+    const uint32_t n = S.n;
+    const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
+    const uint32_t* tc = tile_counts + e.coff / kDelTile;
+    if (threadIdx.x == 0) {
+        uint32_t kept = 0;
+        for (uint32_t t = 0; t < ntiles; ++t) kept += tc[t];
+        s_kept = kept;
+    }
+    __syncthreads();
+    if (s_kept == n) return;  // nothing deleted: the reference returns early (:420-422)
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (threadIdx.x == 0) {
+            uint32_t b = 0;
+            for (uint32_t q = 0; q < t; ++q) b += tc[q];
+            s_base = b;
+        }
+        const uint32_t i = t * kDelTile + threadIdx.x;
+        const uint32_t keep = (i < n) ? flags[e.coff + i] : 0u;
+        const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        const uint32_t ball = __ballot_sync(0xffffffffu, keep);
+        const uint32_t before = __popc(ball & ((1u << lane) - 1u));
+        if (lane == 0) s_warp[wid] = __popc(ball);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int q = 0; q < kDelTile / 32; ++q) {
+                const uint32_t v = s_warp[q];
+                s_warp[q] = acc;
+                acc += v;
+            }
+        }
+        __syncthreads();
+        if (keep) {
+            const uint64_t o = e.coff + s_base + s_warp[wid] + before;
+            stage[0 * total_cap + o] = d.x[i];
+            stage[1 * total_cap + o] = d.z[i];
+            stage[2 * total_cap + o] = d.circ[i];
+            stage[3 * total_cap + o] = d.sigma[i];
+            stage[4 * total_cap + o] = d.u[i];
+            stage[5 * total_cap + o] = d.w[i];
+            stage[6 * total_cap + o] = d.uvs[i];
+            stage[7 * total_cap + o] = d.wvs[i];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_del_copyback(const InstDesc* __restrict__ table, InstState* __restrict__ st,
+                               const ListEntry* __restrict__ list,
+                               const uint32_t* __restrict__ tile_counts,
+                               const double* __restrict__ stage, uint64_t total_cap) {
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const InstState& S = st[e.inst];
+    if (S.status) return;
+    const uint32_t n = S.n;
+    const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
+    const uint32_t* tc = tile_counts + e.coff / kDelTile;
+    __shared__ uint32_t s_kept;
+    if (threadIdx.x == 0) {
+        uint32_t kept = 0;
+        for (uint32_t t = 0; t < ntiles; ++t) kept += tc[t];
+        s_kept = kept;
+    }
+    __syncthreads();
+    const uint32_t kept = s_kept;
+    if (kept == n) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kept; i += gridDim.x * blockDim.x) {
+        const uint64_t o = e.coff + i;
+        d.x[i] = stage[0 * total_cap + o];
+        d.z[i] = stage[1 * total_cap + o];
+        d.circ[i] = stage[2 * total_cap + o];
+        d.sigma[i] = stage[3 * total_cap + o];
+        d.u[i] = stage[4 * total_cap + o];
+        d.w[i] = stage[5 * total_cap + o];
+        d.uvs[i] = stage[6 * total_cap + o];
+        d.wvs[i] = stage[7 * total_cap + o];
+        d.id[i] = i;  // IDs renumbered 0..k-1 (src/VortexSheet.cpp:429)
+    }
+}
+
+__global__ void k_del_finish(InstState* __restrict__ st, const ListEntry* __restrict__ list,
+                             int nlist, const uint32_t* __restrict__ tile_counts) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nlist) return;
+    const ListEntry e = list[k];
+    InstState& S = st[e.inst];
+    if (S.status) return;
+    const uint32_t ntiles = (S.n + kDelTile - 1) / kDelTile;
+    uint32_t kept = 0;
+    for (uint32_t t = 0; t < ntiles; ++t) kept += tile_counts[e.coff / kDelTile + t];
+    S.n = kept;
+}
+
+size_t contour_smem(int max_np) { return sizeof(double) * (4 * (size_t)max_np + 2); }
+
+}  // namespace
+
+void diffuse(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+             const Workspace& ws, int sms, cudaStream_t s) {
+    (void)ws;
+    dim3 g(std::max(1, sms * 8 / std::max(1, nlist)), nlist);
+    k_diffuse<<<g, 256, 0, s>>>(table, st, list, nlist);
+}
+
+void release(const InstDesc* table, InstState* st, const ListEntry* list, int nlist, int max_np,
+             cudaStream_t s) {
+    k_release<<<nlist, kRelThreads, sizeof(double) * 2 * max_np, s>>>(table, st, list);
+}
+
+void reflect(const InstDesc* table, InstState* st, const ListEntry* list, int nlist, int max_np,
+             const Workspace& ws, int sms, cudaStream_t s) {
+    const size_t smem = contour_smem(max_np);
+    static bool attr = false;  // set once, before any graph capture (first call is eager)
+    if (!attr) {
+        cudaFuncSetAttribute(k_reflect, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    cudaMemsetAsync(ws.work + 2, 0, sizeof(unsigned), s);
+    k_reflect<<<sms * 4, 256, smem, s>>>(table, st, list, nlist, ws.work + 2);
+}
+
+void delete_inside(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                   int max_np, const Workspace& ws, int sms, cudaStream_t s) {
+    const size_t smem = contour_smem(max_np);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_del_flags, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr = true;
+    }
+    const int gx = std::max(1, sms * 4 / std::max(1, nlist));
+    k_del_flags<<<dim3(gx, nlist), 256, smem, s>>>(table, st, list, ws.flags, ws.tile_counts);
+    k_del_compact<<<dim3(gx, nlist), kDelTile, 0, s>>>(table, st, list, ws.flags, ws.tile_counts,
+                                                       ws.compact, ws.total_cap);
+    k_del_copyback<<<dim3(gx, nlist), 256, 0, s>>>(table, st, list, ws.tile_counts, ws.compact,
+                                                   ws.total_cap);
+    k_del_finish<<<(nlist + 127) / 128, 128, 0, s>>>(st, list, nlist, ws.tile_counts);
+}
+
+}  // namespace dvmk

@@ -1,0 +1,426 @@
+// Vortex-sheet kernels: influence matrix (src/VortexSheet.cpp:104-165), the
+// least-squares panel-strength solve (src/VortexSheet.cpp:214), sheet-on-blob
+// velocity fused with the convection update (src/VortexSheet.cpp:217-273,
+// src/DVMBase.cpp:167-209) and the pressure loads (src/VortexSheet.cpp:487-514).
+//
+// All FP64.  Pair formulas keep the reference's operation order with one
+// rounding per operation (dadd/dmul/...), so they round like the reference
+// compiled without FP contraction.
+//
+// The solve: the reference forms A^T A and A^T b and solves with LAPACK every
+// call.  Here A ((np+1) x np) is factorised ONCE per body by Householder QR on
+// the GPU and the pseudo-inverse P = R^-1 Q^T is kept in HBM; each step is then
+// gamma = P b (a batched GEMV) plus one iterative-refinement step with the FP64
+// residual r = b - A gamma (gamma += P r).  Same least-squares solution, no
+// O(np^3) work per step.
+#include <cfloat>
+
+#include "dvm_device.cuh"
+#include "dvm_internal.h"
+
+namespace dvmk {
+namespace {
+
+// ---- influence matrix -------------------------------------------------------
+__global__ void k_pq(const double* __restrict__ xp, const double* __restrict__ zp,
+                     const double* __restrict__ xc, const double* __restrict__ zc,
+                     const double* __restrict__ ds, const double* __restrict__ theta, int np,
+                     double* __restrict__ p, double* __restrict__ q) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= np) return;
+    double pij, qij;
+    if (i == j) {
+        pij = -1.0;
+        qij = 1.0;
+    } else {
+        const double xci = xc[i], zci = zc[i], thi = theta[i];
+        const double xj = xp[j], zj = zp[j], thj = theta[j], dsj = ds[j];
+        const double dx = dsub(xci, xj), dz = dsub(zci, zj);
+        const double cj = cos(thj), sj = sin(thj);
+        const double c1 = dsub(dmul(-dx, cj), dmul(dz, sj));
+        const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
+        const double c3 = sin(dsub(thi, thj));
+        const double c4 = cos(dsub(thi, thj));
+        const double c5 = dsub(dmul(dx, sj), dmul(dz, cj));
+        const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
+        const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
+        const double a2 = dsub(thi, dmul(2.0, thj));
+        const double c9 = dsub(dmul(dx, cos(a2)), dmul(dz, sin(a2)));
+        qij = dsub(dadd(c4, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
+                   ddiv(dmul(dadd(dmul(c1, c3), dmul(c4, c5)), c7), dsj));
+        pij = dsub(dadd(dmul(dmul(0.5, c4), c6), dmul(c3, c7)), qij);
+    }
+    p[(size_t)i * np + j] = pij;
+    q[(size_t)i * np + j] = qij;
+}
+
+__global__ void k_assemble_A(const double* __restrict__ p, const double* __restrict__ q,
+                             const double* __restrict__ ds, int np, double* __restrict__ A) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y;
+    if (j >= np) return;
+    if (i == np) {
+        A[(size_t)np * np + j] = ds[j];  // Kelvin row (src/VortexSheet.cpp:159-161)
+        return;
+    }
+    const int jm = (j == 0) ? np - 1 : j - 1;
+    A[(size_t)i * np + j] = dmul(-kRpi2, dadd(p[(size_t)i * np + j], q[(size_t)i * np + jm]));
+}
+
+// ---- Householder QR of [A | I] (column-major, m = np+1 rows) -----------------
+__global__ void k_load_aug(const double* __restrict__ A, int np, double* __restrict__ M) {
+    const int m = np + 1, cols = np + m;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)m * cols;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(t / m), r = (int)(t % m);
+        M[t] = (c < np) ? A[(size_t)r * np + c] : (r == c - np ? 1.0 : 0.0);
+    }
+}
+
+__global__ void k_house(double* __restrict__ M, int np, int k, double* __restrict__ v,
+                        double* __restrict__ tau) {
+    const int m = np + 1;
+    __shared__ double s_red[32];
+    double* col = M + (size_t)k * m;
+    double acc = 0.0;
+    for (int i = k + threadIdx.x; i < m; i += blockDim.x) acc = fma(col[i], col[i], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double nrm2 = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) nrm2 += s_red[q];
+        const double x0 = col[k];
+        const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
+        const double v0 = x0 - alpha;
+        const double vn2 = nrm2 - x0 * x0 + v0 * v0;
+        s_red[0] = alpha;
+        s_red[1] = v0;
+        *tau = (vn2 > 0.0) ? 2.0 / vn2 : 0.0;
+    }
+    __syncthreads();
+    const double alpha = s_red[0], v0 = s_red[1];
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        if (i < k) v[i] = 0.0;
+        else if (i == k) v[i] = v0;
+        else v[i] = col[i];
+    }
+    __syncthreads();
+    for (int i = k + threadIdx.x; i < m; i += blockDim.x) col[i] = (i == k) ? alpha : 0.0;
+}
+
+// Apply H = I - tau v v^T to columns k+1 .. np+m-1, one warp per column.
+__global__ void k_house_apply(double* __restrict__ M, int np, int k, const double* __restrict__ v,
+                              const double* __restrict__ tau) {
+    const int m = np + 1, cols = np + m;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int c = k + 1 + warp;
+    if (c >= cols) return;
+    double* col = M + (size_t)c * m;
+    double acc = 0.0;
+    for (int i = k + lane; i < m; i += 32) acc = fma(v[i], col[i], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    const double f = acc * (*tau);
+    for (int i = k + lane; i < m; i += 32) col[i] = fma(-f, v[i], col[i]);
+}
+
+// P[:, c] = R^-1 (Q^T)[0:np, c] for every column c of Q^T; one warp per column,
+// column-oriented back substitution (coalesced reads of R's columns).
+__global__ void k_backsub(const double* __restrict__ M, int np, double* __restrict__ P) {
+    extern __shared__ double s_y[];
+    const int m = np + 1;
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + wl;
+    if (c >= m) return;
+    double* y = s_y + (size_t)wl * np;
+    const double* qt = M + (size_t)(np + c) * m;
+    for (int i = lane; i < np; i += 32) y[i] = qt[i];
+    __syncwarp();
+    for (int i = np - 1; i >= 0; --i) {
+        const double* Rcol = M + (size_t)i * m;  // column i of R
+        const double xi = y[i] / Rcol[i];
+        __syncwarp();
+        for (int j = lane; j < i; j += 32) y[j] = fma(-Rcol[j], xi, y[j]);
+        if (lane == 0) y[i] = xi;
+        __syncwarp();
+    }
+    for (int i = lane; i < np; i += 32) P[(size_t)i * m + c] = y[i];
+}
+
+// ---- per-step solve -------------------------------------------------------------
+// mode 0: gamma = P b; mode 1: gamma += P res
+__global__ void k_gemv_P(const InstDesc* __restrict__ table, const ListEntry* __restrict__ list,
+                         int mode) {
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const int m = d.np + 1;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= d.np) return;
+    const double* pr = d.P + (size_t)row * m;
+    const double* rhs = mode == 0 ? d.b : d.res;
+    double acc = 0.0;
+    for (int c = lane; c < m; c += 32) acc = fma(pr[c], rhs[c], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) d.gamma[row] = (mode == 0) ? acc : d.gamma[row] + acc;
+}
+
+__global__ void k_residual(const InstDesc* __restrict__ table, const ListEntry* __restrict__ list) {
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const int np = d.np;
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row > np) return;
+    const double* ar = d.A + (size_t)row * np;
+    double acc = 0.0;
+    for (int c = lane; c < np; c += 32) acc = fma(ar[c], d.gamma[c], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) d.res[row] = d.b[row] - acc;
+}
+
+// ---- sheet-on-blob velocity (+ convection) -------------------------------------
+__global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restrict__ table,
+                                                        const InstState* __restrict__ st,
+                                                        const ListEntry* __restrict__ list,
+                                                        int nlist, int mode,
+                                                        unsigned* __restrict__ work) {
+    extern __shared__ double s_pan[];  // 8 arrays of max_np
+    __shared__ unsigned s_pre[1025];
+    __shared__ unsigned s_item;
+    __shared__ int s_loaded;
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += (st[list[k].inst].n + 255) / 256;
+        }
+        s_pre[nlist] = acc;
+        s_loaded = -1;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[nlist];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(work, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= total) break;
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const InstDesc& d = table[e.inst];
+        const int np = d.np;
+        double* sxc = s_pan;
+        double* szc = sxc + np;
+        double* sds = szc + np;
+        double* sct = sds + np;
+        double* sst = sct + np;
+        double* sc2 = sst + np;
+        double* ss2 = sc2 + np;
+        double* sg = ss2 + np;
+        if (s_loaded != k) {
+            for (int j = threadIdx.x; j < np; j += blockDim.x) {
+                sxc[j] = d.xc[j];
+                szc[j] = d.zc[j];
+                sds[j] = d.ds[j];
+                sct[j] = d.cth[j];
+                sst[j] = d.sth[j];
+                sc2[j] = d.c2th[j];
+                ss2[j] = d.s2th[j];
+                sg[j] = d.gamma[j];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_loaded = k;
+        const uint32_t n = st[e.inst].n;
+        const uint32_t i = (item - s_pre[k]) * 256 + threadIdx.x;
+        if (i < n) {
+            const double xi = d.x[i], zi = d.z[i];
+            double us = 0.0, ws = 0.0;
+            for (int j = 0; j < np; ++j) {
+                const double dsj = sds[j], ct = sct[j], stt = sst[j];
+                const double dx = dsub(xi, sxc[j]), dz = dsub(zi, szc[j]);
+                const double c1 = dsub(dmul(-dx, ct), dmul(dz, stt));
+                const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
+                const double c5 = dsub(dmul(dx, stt), dmul(dz, ct));
+                const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
+                const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
+                const double c8 = dadd(dmul(dx, ss2[j]), dmul(dz, sc2[j]));
+                const double c9 = dsub(dmul(dx, sc2[j]), dmul(dz, ss2[j]));
+                const double qx = dadd(dadd(-stt, ddiv(dmul(dmul(0.5, c8), c6), dsj)),
+                                       ddiv(dmul(dadd(dmul(c1, ct), dmul(c5, stt)), c7), dsj));
+                const double px = dsub(dsub(dmul(dmul(-0.5, c6), stt), dmul(c7, ct)), qx);
+                const double qy = dadd(dadd(ct, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
+                                       ddiv(dmul(dsub(dmul(c1, stt), dmul(c5, ct)), c7), dsj));
+                const double py = dsub(dsub(dmul(dmul(0.5, c6), ct), dmul(c7, stt)), qy);
+                const double g0 = sg[j], g1 = (j == np - 1) ? sg[0] : sg[j + 1];
+                us = dadd(us, dadd(dmul(px, g0), dmul(qx, g1)));
+                ws = dadd(ws, dadd(dmul(py, g0), dmul(qy, g1)));
+            }
+            const double uvs = dmul(us, kRpi2), wvs = dmul(ws, kRpi2);
+            d.uvs[i] = uvs;
+            d.wvs[i] = wvs;
+            if (mode >= 1) {
+                const double vx = dmul(dadd(dadd(d.u[i], uvs), d.ux), d.dt);
+                const double vz = dmul(dadd(dadd(d.w[i], wvs), d.uz), d.dt);
+                if (mode == 1) {
+                    d.x[i] = dadd(xi, vx);
+                    d.z[i] = dadd(zi, vz);
+                } else {
+                    const int s = mode - 2;
+                    const double a = s == 0 ? 0.0 : (s == 1 ? -17. / 32 : -32. / 27);
+                    const double bb = s == 0 ? 1. / 4 : (s == 1 ? 8. / 9 : 3. / 4);
+                    const double q1o = s == 0 ? 0.0 : d.q1[i];
+                    const double q2o = s == 0 ? 0.0 : d.q2[i];
+                    const double q1 = dadd(dmul(a, q1o), vx);
+                    const double q2 = dadd(dmul(a, q2o), vz);
+                    d.q1[i] = q1;
+                    d.q2[i] = q2;
+                    d.x[i] = dadd(xi, dmul(bb, q1));
+                    d.z[i] = dadd(zi, dmul(bb, q2));
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_convect_update(const InstDesc* __restrict__ table,
+                                 const InstState* __restrict__ st,
+                                 const ListEntry* __restrict__ list, int nlist, int mode) {
+    const ListEntry e = list[blockIdx.y];
+    const InstDesc& d = table[e.inst];
+    const uint32_t n = st[e.inst].n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double vx = dmul(dadd(dadd(d.u[i], d.uvs[i]), d.ux), d.dt);
+        const double vz = dmul(dadd(dadd(d.w[i], d.wvs[i]), d.uz), d.dt);
+        if (mode == 1) {
+            d.x[i] = dadd(d.x[i], vx);
+            d.z[i] = dadd(d.z[i], vz);
+        } else {
+            const int s = mode - 2;
+            const double a = s == 0 ? 0.0 : (s == 1 ? -17. / 32 : -32. / 27);
+            const double bb = s == 0 ? 1. / 4 : (s == 1 ? 8. / 9 : 3. / 4);
+            const double q1 = dadd(dmul(a, s == 0 ? 0.0 : d.q1[i]), vx);
+            const double q2 = dadd(dmul(a, s == 0 ? 0.0 : d.q2[i]), vz);
+            d.q1[i] = q1;
+            d.q2[i] = q2;
+            d.x[i] = dadd(d.x[i], dmul(bb, q1));
+            d.z[i] = dadd(d.z[i], dmul(bb, q2));
+        }
+    }
+}
+
+// ---- loads (src/VortexSheet.cpp:489-513), one block per simulation ---------------
+__global__ void k_loads(const InstDesc* __restrict__ table, InstState* __restrict__ st,
+                        const ListEntry* __restrict__ list) {
+    extern __shared__ double s_P[];
+    const ListEntry e = list[blockIdx.x];
+    const InstDesc& d = table[e.inst];
+    const int np = d.np;
+    if (threadIdx.x != 0) return;
+    const double c = ddiv(-d.rho, d.dt);
+    s_P[0] = 0.0;
+    for (int i = 0; i < np - 1; ++i) s_P[i + 1] = dadd(s_P[i], dmul(c, dmul(d.gamma[i], d.ds[i])));
+    for (int i = 0; i < np - 1; ++i) s_P[i] = dmul(0.5, dadd(s_P[i], s_P[i + 1]));
+    s_P[np - 1] = dmul(0.5, dadd(s_P[np - 1], s_P[0]));
+    double pmax = s_P[0];
+    for (int i = 1; i < np; ++i)
+        if (s_P[i] > pmax) pmax = s_P[i];
+    const double pref = dmul(dmul(dmul(0.5, d.rho), d.Ur), d.Ur);
+    const double shift = dmul(dsub(pref, pmax), 1.0);
+    double sx = 0.0, sz = 0.0;
+    for (int i = 0; i < np; ++i) {
+        const double Pi = dadd(s_P[i], shift);
+        sx = dadd(sx, dmul(dmul(Pi, d.enx[i]), d.ds[i]));
+        sz = dadd(sz, dmul(dmul(Pi, d.enz[i]), d.ds[i]));
+    }
+    const double fx = -sx, fz = -sz;
+    const double den = dmul(dmul(dmul(dmul(0.5, d.rho), d.area), d.Ur), d.Ur);
+    InstState& s = st[e.inst];
+    s.fx = fx;
+    s.fz = fz;
+    s.cd = ddiv(fx, den);
+    s.cl = ddiv(fz, den);
+}
+
+__global__ void k_step_counter(InstState* __restrict__ st, const ListEntry* __restrict__ list,
+                               int nlist) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < nlist) st[list[k].inst].step += 1;
+}
+
+}  // namespace
+
+void influence_matrix(const double* xp, const double* zp, const double* xc, const double* zc,
+                      const double* ds, const double* theta, int np, double* pq_scratch,
+                      double* A, cudaStream_t s) {
+    double* p = pq_scratch;
+    double* q = pq_scratch + (size_t)np * np;
+    dim3 g((np + 127) / 128, np);
+    k_pq<<<g, 128, 0, s>>>(xp, zp, xc, zc, ds, theta, np, p, q);
+    dim3 g2((np + 127) / 128, np + 1);
+    k_assemble_A<<<g2, 128, 0, s>>>(p, q, ds, np, A);
+}
+
+size_t pseudo_inverse_work_doubles(int np) {
+    const size_t m = (size_t)np + 1;
+    return m * (np + m) + m + 8;
+}
+
+void pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s) {
+    const int m = np + 1, cols = np + m;
+    double* M = work;
+    double* v = M + (size_t)m * cols;
+    double* tau = v + m;
+    k_load_aug<<<256, 256, 0, s>>>(A, np, M);
+    for (int k = 0; k < np; ++k) {
+        k_house<<<1, 256, 0, s>>>(M, np, k, v, tau);
+        const int ncols = cols - (k + 1);
+        const int threads = 256, wpb = threads / 32;
+        k_house_apply<<<(ncols + wpb - 1) / wpb, threads, 0, s>>>(M, np, k, v, tau);
+    }
+    // warps per block such that the per-warp right-hand sides fit 48 KB of shared memory
+    const int wpb = std::max(1, std::min(4, (int)(48 * 1024 / (sizeof(double) * np))));
+    k_backsub<<<(m + wpb - 1) / wpb, wpb * 32, sizeof(double) * np * wpb, s>>>(M, np, P);
+}
+
+void sheet_solve(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                 int max_np, cudaStream_t s) {
+    (void)st;
+    const int rows_per_block = 8;
+    dim3 g((max_np + 1 + rows_per_block - 1) / rows_per_block, nlist);
+    k_gemv_P<<<g, rows_per_block * 32, 0, s>>>(table, list, 0);
+    // One refinement step with the FP64 residual of the full (np+1)-row system.
+    k_residual<<<g, rows_per_block * 32, 0, s>>>(table, list);
+    k_gemv_P<<<g, rows_per_block * 32, 0, s>>>(table, list, 1);
+}
+
+void sheet_velocity(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                    int mode, int max_np, const Workspace& ws, int sms, cudaStream_t s) {
+    const size_t smem = sizeof(double) * 8 * (size_t)max_np;
+    static bool attr = false;  // set once, before any graph capture (first call is eager)
+    if (!attr) {
+        cudaFuncSetAttribute(k_sheet_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024);
+        attr = true;
+    }
+    cudaMemsetAsync(ws.work + 1, 0, sizeof(unsigned), s);
+    k_sheet_velocity<<<sms * 4, 256, smem, s>>>(table, st, list, nlist, mode, ws.work + 1);
+}
+
+void convect_update(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
+                    int mode, const Workspace& ws, int sms, cudaStream_t s) {
+    (void)ws;
+    dim3 g(std::max(1, sms * 4 / std::max(1, nlist)), nlist);
+    k_convect_update<<<g, 256, 0, s>>>(table, st, list, nlist, mode);
+}
+
+void loads(const InstDesc* table, InstState* st, const ListEntry* list, int nlist, int max_np,
+           cudaStream_t s) {
+    k_loads<<<nlist, 32, sizeof(double) * max_np, s>>>(table, st, list);
+}
+
+void step_counter(InstState* st, const ListEntry* list, int nlist, cudaStream_t s) {
+    k_step_counter<<<(nlist + 127) / 128, 128, 0, s>>>(st, list, nlist);
+}
+
+}  // namespace dvmk

@@ -1,0 +1,351 @@
+"""ctypes binding of the C ABI in include/dvm_cuda.h (libdvm_cuda.so).
+
+This is the Python face of the drop-in boundary: it calls exactly the entry
+points a cgo / JNI / ctypes user would bind.  There is no fallback: if the
+CUDA library is missing, or no B200 is visible, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libdvm_cuda.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "dvm_cuda.h")
+
+OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_CAPACITY, ERR_RELEASE, ERR_STATE, ERR_RNG, ERR_NO_DEVICE = range(10)
+F64, F32 = 0, 1
+EULER, RK3 = 0, 1
+DELETE, ABSORB, REFLECT = 0, 1, 2
+RNG_INJECT, RNG_PHILOX = 0, 1
+PROF_FAMILIES = ["nbody", "rhs", "solve", "sheetvel", "diffuse_release", "cross", "loads", "sort",
+                 "step"]
+(PHASE_BIOTSAVART, PHASE_SOLVE, PHASE_SHEETBC, PHASE_CONVECT, PHASE_DIFFUSE, PHASE_RELEASE,
+ PHASE_CROSS, PHASE_LOADS, PHASE_INCREMENT, PHASE_REFLECT, PHASE_DELETE) = range(11)
+
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+
+
+class DvmError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class Particle(C.Structure):
+    _fields_ = [("x", C.c_double), ("z", C.c_double), ("circ", C.c_double), ("sigma", C.c_double)]
+
+
+class Velocity(C.Structure):
+    _fields_ = [("u", C.c_double), ("w", C.c_double)]
+
+
+class SimParams(C.Structure):
+    _fields_ = [
+        ("rho", C.c_double), ("nu", C.c_double), ("dt", C.c_double), ("ux", C.c_double),
+        ("uz", C.c_double), ("cutoff_exp", C.c_double), ("max_numpanelvort", C.c_uint32),
+        ("scheme", C.c_int32), ("surface_cross", C.c_int32), ("rng", C.c_int32),
+        ("precision", C.c_int32), ("reserved", C.c_int32), ("seed", C.c_int64),
+        ("capacity", C.c_uint64), ("rng_capacity", C.c_uint64),
+    ]
+
+
+# name -> (restype, argtypes); every symbol declared in include/dvm_cuda.h
+SIGNATURES = {
+    "dvm_abi_version": (C.c_int, []),
+    "dvm_status_string": (C.c_char_p, [C.c_int]),
+    "dvm_last_error": (C.c_char_p, []),
+    "dvm_ctx_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "dvm_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "dvm_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "dvm_ctx_memory": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "dvm_ctx_device_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "dvm_ctx_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "dvm_sim_bytes": (C.c_int, [C.POINTER(SimParams), C.c_int, C.POINTER(C.c_uint64)]),
+    "dvm_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "dvm_ctx_profile": (C.c_int, [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_uint64)]),
+    "dvm_ctx_profile_reset": (C.c_int, [C.c_void_p]),
+    "dvm_biot_savart_self": (C.c_int, [C.c_void_p, C.POINTER(Particle), C.c_uint64, C.POINTER(Velocity), C.c_int]),
+    "dvm_biot_savart_at": (C.c_int, [C.c_void_p, C.POINTER(Particle), C.c_uint64, _dp, _dp, C.c_uint64,
+                                     C.POINTER(Velocity), C.c_int]),
+    "dvm_biot_savart_self_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int]),
+    "dvm_biot_savart_at_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2
+                                  + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int, C.c_int]),
+    "dvm_sim_create": (C.c_int, [C.c_void_p, C.POINTER(SimParams), _dp, _dp, C.c_int, C.POINTER(C.c_void_p)]),
+    "dvm_sim_destroy": (C.c_int, [C.c_void_p]),
+    "dvm_sim_set_blobs": (C.c_int, [C.c_void_p, C.c_uint64, _dp, _dp, _dp, _dp]),
+    "dvm_sim_get_blobs": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)] + [_dp] * 8 + [_u32p]),
+    "dvm_sim_num_blobs": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "dvm_sim_num_panels": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "dvm_sim_get_gamma": (C.c_int, [C.c_void_p, _dp]),
+    "dvm_sim_set_gamma": (C.c_int, [C.c_void_p, _dp]),
+    "dvm_sim_get_rhs": (C.c_int, [C.c_void_p, _dp]),
+    "dvm_sim_get_influence": (C.c_int, [C.c_void_p, _dp]),
+    "dvm_sim_get_panels": (C.c_int, [C.c_void_p] + [_dp] * 6),
+    "dvm_sim_get_loads": (C.c_int, [C.c_void_p] + [_dp] * 4),
+    "dvm_sim_get_step": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32)]),
+    "dvm_sim_push_uniforms": (C.c_int, [C.c_void_p, _dp, C.c_uint64]),
+    "dvm_sim_rng_position": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "dvm_sim_status": (C.c_int, [C.c_void_p]),
+    "dvm_sim_clear_status": (C.c_int, [C.c_void_p]),
+    "dvm_sim_phase": (C.c_int, [C.c_void_p, C.c_int]),
+    "dvm_sim_step": (C.c_int, [C.c_void_p, C.c_int]),
+    "dvm_step_batch": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int]),
+}
+
+_LIB = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libdvm_cuda.so (raises if it is absent: there is no CPU path)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing; build it with `python -m dvmpp_b200.build`")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise DvmError(rc, _LIB.dvm_last_error().decode(errors="replace"))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class Context:
+    """One device, one stream, an HBM budget (dvm_ctx)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        _check(self.lib.dvm_ctx_create(device, budget_bytes, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dvm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def sync(self):
+        _check(self.lib.dvm_ctx_synchronize(self.h))
+
+    def memory(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(self.lib.dvm_ctx_memory(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def device_info(self):
+        s, ma, mi = C.c_int(), C.c_int(), C.c_int()
+        _check(self.lib.dvm_ctx_device_info(self.h, C.byref(s), C.byref(ma), C.byref(mi)))
+        return s.value, ma.value, mi.value
+
+    def set_profiling(self, on: bool):
+        _check(self.lib.dvm_ctx_set_profiling(self.h, 1 if on else 0))
+
+    def profile(self):
+        """{family: (total ms, timed launches)} from CUDA events on the ctx stream."""
+        out = {}
+        for k, name in enumerate(PROF_FAMILIES):
+            ms, n = C.c_double(), C.c_uint64()
+            _check(self.lib.dvm_ctx_profile(self.h, k, C.byref(ms), C.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
+    def profile_reset(self):
+        _check(self.lib.dvm_ctx_profile_reset(self.h))
+
+    def launches(self) -> int:
+        v = C.c_uint64()
+        _check(self.lib.dvm_ctx_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    # ---- VelocityKernel plugin seam
+    def biot_savart_self(self, x, z, circ, sigma, precision=F32):
+        n = len(x)
+        p = (Particle * max(n, 1))()
+        arr = np.frombuffer(p, dtype=np.float64, count=4 * n).reshape(n, 4) if n else None
+        if n:
+            arr[:, 0], arr[:, 1], arr[:, 2], arr[:, 3] = x, z, circ, sigma
+        out = (Velocity * max(n, 1))()
+        _check(self.lib.dvm_biot_savart_self(self.h, p, n, out, precision))
+        v = np.frombuffer(out, dtype=np.float64, count=2 * n).reshape(n, 2) if n else np.zeros((0, 2))
+        return v[:, 0].copy(), v[:, 1].copy()
+
+    def biot_savart_at(self, x, z, circ, sigma, tx, tz, precision=F32):
+        n = len(x)
+        p = (Particle * max(n, 1))()
+        if n:
+            arr = np.frombuffer(p, dtype=np.float64, count=4 * n).reshape(n, 4)
+            arr[:, 0], arr[:, 1], arr[:, 2], arr[:, 3] = x, z, circ, sigma
+        tx, tz = _f64(tx), _f64(tz)
+        nt = tx.size
+        out = (Velocity * max(nt, 1))()
+        _check(self.lib.dvm_biot_savart_at(self.h, p, n, _p(tx), _p(tz), nt, out, precision))
+        v = np.frombuffer(out, dtype=np.float64, count=2 * nt).reshape(nt, 2) if nt else np.zeros((0, 2))
+        return v[:, 0].copy(), v[:, 1].copy()
+
+    def step_batch(self, sims, nsteps=1, use_graph=True):
+        arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
+        _check(self.lib.dvm_step_batch(self.h, arr, len(sims), nsteps, 1 if use_graph else 0))
+
+    def sim(self, params: "Params", xp, zp) -> "Simulation":
+        return Simulation(self, params, xp, zp)
+
+
+@dataclass
+class Params:
+    rho: float = 1.0
+    nu: float = 1e-3
+    dt: float = 0.005
+    ux: float = 3.0
+    uz: float = 0.0
+    cutoff_exp: float = 0.675
+    max_numpanelvort: int = 3
+    scheme: int = EULER
+    surface_cross: int = REFLECT
+    rng: int = RNG_INJECT
+    precision: int = F64
+    seed: int = 1
+    capacity: int = 1 << 16
+    rng_capacity: int = 1 << 20
+
+    def c(self) -> SimParams:
+        return SimParams(self.rho, self.nu, self.dt, self.ux, self.uz, self.cutoff_exp,
+                         self.max_numpanelvort, self.scheme, self.surface_cross, self.rng,
+                         self.precision, 0, self.seed, self.capacity, self.rng_capacity)
+
+
+def sim_bytes(params: Params, npanels: int) -> int:
+    lib = load()
+    b = C.c_uint64()
+    cp = params.c()
+    _check(lib.dvm_sim_bytes(C.byref(cp), npanels, C.byref(b)))
+    return b.value
+
+
+class Simulation:
+    """One simulation resident on the device (dvm_sim)."""
+
+    def __init__(self, ctx: Context, params: Params, xp, zp):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.params = params
+        xp, zp = _f64(xp), _f64(zp)
+        h = C.c_void_p()
+        cp = params.c()
+        _check(self.lib.dvm_sim_create(ctx.h, C.byref(cp), _p(xp), _p(zp), xp.size, C.byref(h)))
+        self.h = h
+        self.np = xp.size - 1
+
+    def close(self):
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
+            self.lib.dvm_sim_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_blobs(self, x, z, circ, sigma):
+        x, z, circ, sigma = map(_f64, (x, z, circ, sigma))
+        _check(self.lib.dvm_sim_set_blobs(self.h, x.size, _p(x), _p(z), _p(circ), _p(sigma)))
+
+    @property
+    def n(self) -> int:
+        v = C.c_uint64()
+        _check(self.lib.dvm_sim_num_blobs(self.h, C.byref(v)))
+        return v.value
+
+    def blobs(self):
+        n = self.n
+        arrs = [np.empty(n) for _ in range(8)]
+        ids = np.empty(n, dtype=np.uint32)
+        nn = C.c_uint64()
+        _check(self.lib.dvm_sim_get_blobs(self.h, n, C.byref(nn), *[_p(a) for a in arrs],
+                                          ids.ctypes.data_as(_u32p)))
+        d = dict(zip(["x", "z", "circ", "sigma", "u", "w", "uvs", "wvs"], arrs))
+        d["id"] = ids
+        return d
+
+    def gamma(self):
+        g = np.empty(self.np)
+        _check(self.lib.dvm_sim_get_gamma(self.h, _p(g)))
+        return g
+
+    def set_gamma(self, g):
+        g = _f64(g)
+        _check(self.lib.dvm_sim_set_gamma(self.h, _p(g)))
+
+    def rhs(self):
+        b = np.empty(self.np + 1)
+        _check(self.lib.dvm_sim_get_rhs(self.h, _p(b)))
+        return b
+
+    def influence(self):
+        A = np.empty((self.np + 1, self.np))
+        _check(self.lib.dvm_sim_get_influence(self.h, _p(A)))
+        return A
+
+    def panels(self):
+        arrs = [np.empty(self.np) for _ in range(6)]
+        _check(self.lib.dvm_sim_get_panels(self.h, *[_p(a) for a in arrs]))
+        return dict(zip(["xc", "zc", "ds", "theta", "enx", "enz"], arrs))
+
+    def loads(self):
+        v = [C.c_double() for _ in range(4)]
+        _check(self.lib.dvm_sim_get_loads(self.h, *[C.byref(a) for a in v]))
+        return tuple(a.value for a in v)  # fx, fz, cd, cl
+
+    def step_number(self) -> int:
+        v = C.c_uint32()
+        _check(self.lib.dvm_sim_get_step(self.h, C.byref(v)))
+        return v.value
+
+    def push_uniforms(self, u):
+        u = _f64(u)
+        _check(self.lib.dvm_sim_push_uniforms(self.h, _p(u), u.size))
+
+    def rng_position(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(self.lib.dvm_sim_rng_position(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def status(self) -> int:
+        return self.lib.dvm_sim_status(self.h)
+
+    def check(self):
+        _check(self.lib.dvm_sim_status(self.h))
+
+    def clear_status(self):
+        _check(self.lib.dvm_sim_clear_status(self.h))
+
+    def phase(self, k: int):
+        _check(self.lib.dvm_sim_phase(self.h, k))
+
+    def step(self, nsteps: int = 1):
+        _check(self.lib.dvm_sim_step(self.h, nsteps))

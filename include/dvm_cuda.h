@@ -1,0 +1,202 @@
+/* dvm_cuda.h -- C ABI of libdvm_cuda.so, the B200 (sm_100a) implementation of
+ * the DVMpp per-step hot path.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or C++ types cross
+ * this boundary.  Every entry point returns a status code (DVM_OK == 0) and
+ * never throws; dvm_last_error() gives the message of the calling thread's
+ * last failure.  The C++ drop-in classes (dvmpp_b200/host) map statuses to the
+ * reference's dvm:: exceptions (src/Exceptions.hpp:13-81).
+ *
+ * Reference interfaces replaced (gdeskos/DVMpp, file:line):
+ *   dvm_biot_savart_self      DirectKernel::computeSelfInduced  src/VelocityKernel.cpp:30-67
+ *   dvm_biot_savart_at        DirectKernel::computeInducedAt    src/VelocityKernel.cpp:69-109
+ *   dvm_sim_create            VortexSheet(xml, stamp) set-up    src/VortexSheet.cpp:12-54,78-165
+ *   dvm_sim_set_blobs /
+ *   dvm_sim_get_blobs         VortexBlobs public SoA members    src/VortexBlobs.hpp:24-32
+ *   dvm_sim_phase(BIOTSAVART) VortexBlobs::biotsavart           src/VortexBlobs.cpp:229-249
+ *   dvm_sim_phase(SOLVE)      VortexSheet::solvevortexsheet     src/VortexSheet.cpp:167-215
+ *   dvm_sim_phase(SHEETBC)    VortexSheet::vortexsheetbc        src/VortexSheet.cpp:217-273
+ *   dvm_sim_phase(CONVECT)    DVMBase::convect                  src/DVMBase.cpp:167-209
+ *   dvm_sim_phase(DIFFUSE)    VortexBlobs::diffusion_random_walk src/VortexBlobs.cpp:251-265
+ *   dvm_sim_phase(RELEASE)    release_nascent_vortices_rw + append_vortices
+ *                                                               src/VortexSheet.cpp:275-333,
+ *                                                               src/VortexBlobs.cpp:211-227
+ *   dvm_sim_phase(CROSS)      surface-crossing dispatch         src/DVMBase.cpp:107-118
+ *   dvm_sim_phase(REFLECT)    VortexSheet::reflect              src/VortexSheet.cpp:345-405
+ *   dvm_sim_phase(DELETE)     VortexSheet::delete_inside        src/VortexSheet.cpp:407-445
+ *   dvm_sim_phase(LOADS)      VortexSheet::compute_loads        src/VortexSheet.cpp:487-514
+ *   dvm_sim_step              DVMBase::compute_step (+increment_step)
+ *                                                               src/DVMBase.cpp:86-133,145-149
+ *   dvm_sim_push_uniforms     Random::rand stream feed          src/Random.cpp:8-18
+ *   dvm_step_batch            (no counterpart: many simulations per launch)
+ */
+#ifndef DVM_CUDA_H
+#define DVM_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DVM_ABI_VERSION 1
+
+/* status codes */
+#define DVM_OK 0
+#define DVM_ERR_ARG 1        /* bad argument (null pointer, size mismatch, bad enum) */
+#define DVM_ERR_OOM 2        /* device allocation failed or HBM budget exceeded */
+#define DVM_ERR_CUDA 3       /* CUDA runtime error (message in dvm_last_error) */
+#define DVM_ERR_TIMEOUT 4    /* bounded device wait ran out (reserved) */
+#define DVM_ERR_CAPACITY 5   /* a release would exceed the simulation's blob capacity */
+#define DVM_ERR_RELEASE 6    /* release count not > 1e-15 (reference throws VortexException) */
+#define DVM_ERR_STATE 7      /* call not valid in the current state */
+#define DVM_ERR_RNG 8        /* injected uniform stream exhausted */
+#define DVM_ERR_NO_DEVICE 9  /* no CUDA device / library built for another GPU */
+
+/* arithmetic of the pair interactions */
+#define DVM_F64 0 /* FP64, reference operation order */
+#define DVM_F32 1 /* FP32 with compensated sums (sheet-on-blob stays FP64) */
+
+#define DVM_EULER 0 /* Scheme::Euler, src/DVMBase.hpp:27-30 */
+#define DVM_RK3 1   /* Scheme::RK3 */
+
+#define DVM_DELETE 0  /* SurfaceCross, src/DVMBase.hpp:33-41 */
+#define DVM_ABSORB 1  /* falls back to REFLECT as in src/DVMBase.cpp:111-114 */
+#define DVM_REFLECT 2
+
+#define DVM_RNG_INJECT 0 /* uniforms supplied by the host (reference mt19937 stream) */
+#define DVM_RNG_PHILOX 1 /* counter-based Philox4x32-10 on the device */
+
+/* phases of DVMBase::compute_step, for dvm_sim_phase */
+#define DVM_PHASE_BIOTSAVART 0
+#define DVM_PHASE_SOLVE 1
+#define DVM_PHASE_SHEETBC 2
+#define DVM_PHASE_CONVECT 3
+#define DVM_PHASE_DIFFUSE 4
+#define DVM_PHASE_RELEASE 5
+#define DVM_PHASE_CROSS 6
+#define DVM_PHASE_LOADS 7
+#define DVM_PHASE_INCREMENT 8
+#define DVM_PHASE_REFLECT 9
+#define DVM_PHASE_DELETE 10
+
+typedef struct dvm_ctx dvm_ctx; /* one device, one stream, a workspace, a table of sims */
+typedef struct dvm_sim dvm_sim; /* one simulation resident in the ctx's HBM budget */
+
+/* Same layout as dvm::VortexParticle / dvm::VelocityResult (src/VelocityKernel.hpp:15-26). */
+typedef struct {
+    double x, z, circ, sigma;
+} dvm_particle;
+typedef struct {
+    double u, w;
+} dvm_velocity;
+
+/* XML parameters the hot path reads (src/XmlHandler.cpp:162-202) plus device options. */
+typedef struct {
+    double rho;            /* constants/density */
+    double nu;             /* constants/nu */
+    double dt;             /* time/dt */
+    double ux, uz;         /* flow/ux, flow/uz */
+    double cutoff_exp;     /* constants/cutoff_exp */
+    uint32_t max_numpanelvort; /* constants/max_NumPanelVort */
+    int32_t scheme;        /* DVM_EULER | DVM_RK3 */
+    int32_t surface_cross; /* DVM_DELETE | DVM_ABSORB | DVM_REFLECT */
+    int32_t rng;           /* DVM_RNG_INJECT | DVM_RNG_PHILOX */
+    int32_t precision;     /* DVM_F64 | DVM_F32 */
+    int32_t reserved;
+    int64_t seed;          /* constants/seed (Philox key) */
+    uint64_t capacity;     /* maximum number of blobs held on the device */
+    uint64_t rng_capacity; /* inject mode: uniforms held on the device at once */
+} dvm_sim_params;
+
+int dvm_abi_version(void);
+const char* dvm_status_string(int status);
+const char* dvm_last_error(void);
+
+/* ---- context ---------------------------------------------------------------- */
+/* hbm_budget_bytes == 0: 90 % of the device's free memory. */
+int dvm_ctx_create(int device, uint64_t hbm_budget_bytes, dvm_ctx** out);
+int dvm_ctx_destroy(dvm_ctx* ctx);
+int dvm_ctx_synchronize(dvm_ctx* ctx);
+int dvm_ctx_memory(dvm_ctx* ctx, uint64_t* in_use, uint64_t* budget);
+int dvm_ctx_device_info(dvm_ctx* ctx, int* sms, int* cc_major, int* cc_minor);
+/* Kernel launches issued so far by this context (graph replays count every
+ * kernel node of the graph). */
+int dvm_ctx_launch_count(dvm_ctx* ctx, uint64_t* launches);
+/* Per-kernel-family device time, measured with CUDA events recorded on the
+ * ctx stream around each launch while profiling is on (steps then run without
+ * graph capture).  dvm_ctx_profile synchronises and returns the total
+ * milliseconds and the number of timed launches of one family. */
+#define DVM_PROF_NBODY 0      /* self-induced pair kernel only */
+#define DVM_PROF_RHS 1        /* blob-on-collocation right-hand side */
+#define DVM_PROF_SOLVE 2      /* gamma = P b + refinement */
+#define DVM_PROF_SHEETVEL 3   /* sheet-on-blob velocity + convection update */
+#define DVM_PROF_DIFFREL 4    /* diffusion + release/append */
+#define DVM_PROF_CROSS 5      /* reflect / delete */
+#define DVM_PROF_LOADS 6      /* loads + step counter */
+#define DVM_PROF_SORT 7       /* Morton sort, pack, partial combine */
+#define DVM_PROF_STEP 8       /* whole step */
+#define DVM_PROF_FAMILIES 9
+int dvm_ctx_set_profiling(dvm_ctx* ctx, int on);
+int dvm_ctx_profile(dvm_ctx* ctx, int family, double* ms_total, uint64_t* launches);
+int dvm_ctx_profile_reset(dvm_ctx* ctx);
+/* Bytes a simulation with these parameters and np panels occupies. */
+int dvm_sim_bytes(const dvm_sim_params* p, int npanels, uint64_t* bytes);
+
+/* ---- VelocityKernel plugin seam (host AoS in, host AoS out) ------------------------ */
+int dvm_biot_savart_self(dvm_ctx* ctx, const dvm_particle* p, uint64_t n, dvm_velocity* out,
+                         int precision);
+int dvm_biot_savart_at(dvm_ctx* ctx, const dvm_particle* src, uint64_t ns, const double* tx,
+                       const double* tz, uint64_t nt, dvm_velocity* out, int precision);
+/* Device-resident SoA variants (pointers from cudaMalloc); asynchronous on the
+ * ctx stream.  skip_close: 1 skips pairs with r^2 <= 1e-15 like computeInducedAt. */
+int dvm_biot_savart_self_device(dvm_ctx* ctx, const double* x, const double* z,
+                                const double* circ, const double* sigma, uint64_t n, double* u,
+                                double* w, int precision);
+int dvm_biot_savart_at_device(dvm_ctx* ctx, const double* x, const double* z, const double* circ,
+                              const double* sigma, uint64_t ns, const double* tx,
+                              const double* tz, uint64_t nt, double* u, double* w,
+                              int precision, int skip_close);
+
+/* ---- simulations ---------------------------------------------------------------- */
+/* body_x/body_z: closed CCW contour of npoints (first point repeated last),
+ * the reference's domain_file format (src/VortexSheet.cpp:56-76). */
+int dvm_sim_create(dvm_ctx* ctx, const dvm_sim_params* p, const double* body_x,
+                   const double* body_z, int npoints, dvm_sim** out);
+int dvm_sim_destroy(dvm_sim* sim);
+int dvm_sim_set_blobs(dvm_sim* sim, uint64_t n, const double* x, const double* z,
+                      const double* circ, const double* sigma);
+/* Any output pointer may be NULL.  Fails with DVM_ERR_ARG if cap < n. */
+int dvm_sim_get_blobs(dvm_sim* sim, uint64_t cap, uint64_t* n, double* x, double* z,
+                      double* circ, double* sigma, double* u, double* w, double* uvs,
+                      double* wvs, uint32_t* id);
+int dvm_sim_num_blobs(dvm_sim* sim, uint64_t* n);
+int dvm_sim_num_panels(dvm_sim* sim, int* np);
+int dvm_sim_get_gamma(dvm_sim* sim, double* gamma);
+int dvm_sim_set_gamma(dvm_sim* sim, const double* gamma);
+int dvm_sim_get_rhs(dvm_sim* sim, double* b);             /* np+1 */
+int dvm_sim_get_influence(dvm_sim* sim, double* A);       /* (np+1) x np, row-major */
+int dvm_sim_get_panels(dvm_sim* sim, double* xc, double* zc, double* ds, double* theta,
+                       double* enx, double* enz);
+int dvm_sim_get_loads(dvm_sim* sim, double* fx, double* fz, double* cd, double* cl);
+int dvm_sim_get_step(dvm_sim* sim, uint32_t* step);
+/* Inject mode: append uniforms in (0,1) to the device stream (in draw order). */
+int dvm_sim_push_uniforms(dvm_sim* sim, const double* u, uint64_t n);
+int dvm_sim_rng_position(dvm_sim* sim, uint64_t* consumed_total, uint64_t* available);
+/* First error raised on the device for this simulation (synchronises). */
+int dvm_sim_status(dvm_sim* sim);
+int dvm_sim_clear_status(dvm_sim* sim);
+int dvm_sim_phase(dvm_sim* sim, int phase);
+int dvm_sim_step(dvm_sim* sim, int nsteps);
+
+/* ---- batches ---------------------------------------------------------------------- */
+/* Advance every listed simulation by nsteps; each kernel of the step serves all
+ * of them in one launch.  use_graph != 0 captures the step in a CUDA graph
+ * (re-used while the list is unchanged).  Asynchronous: check dvm_sim_status. */
+int dvm_step_batch(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int nsteps, int use_graph);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DVM_CUDA_H */

@@ -1,0 +1,148 @@
+"""Biot-Savart parity on the GPU, through the C ABI (include/dvm_cuda.h).
+
+Oracle: the C restatement of src/VelocityKernel.cpp:30-109 (oracle/dvm_oracle.c).
+Tolerances:
+  * DVM_F64: |u - u_oracle| <= 1e-12 * max|u_oracle| (same operation order; only
+    exp() may differ by an ulp and chunk partial sums re-associate).
+  * DVM_F32: relative L2 error <= 1e-5 (the bar for the FP32 compensated path),
+    max-norm error reported.
+Cases follow the reference's own tests (tests/unit/test_VelocityKernel.cpp,
+tests/integration/test_BiotSavart.cpp) plus seeded random sets.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from dvmpp_b200 import native as N
+from dvmpp_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+F64_TOL = 1e-12
+F32_REL_L2 = 1e-5
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_empty_and_single(ctx):
+    # test_VelocityKernel.cpp:47-71
+    u, w = ctx.biot_savart_self([], [], [], [], N.F64)
+    assert u.size == 0 and w.size == 0
+    for prec in (N.F64, N.F32):
+        u, w = ctx.biot_savart_self([0.0], [0.0], [1.0], [0.1], prec)
+        assert u[0] == 0.0 and w[0] == 0.0
+
+
+@pytest.mark.parametrize("prec", [N.F64, N.F32])
+def test_vortex_pair_analytic(ctx, prec):
+    # test_VelocityKernel.cpp:99-125 and test_BiotSavart.cpp:15-51
+    d, G, s = 2.0, 1.0, 0.01
+    u, w = ctx.biot_savart_self([-d / 2, d / 2], [0, 0], [G, -G], [s, s], prec)
+    expected = G / (2 * math.pi * d)
+    assert abs(w[0] - expected) <= 0.01 * expected
+    assert abs(w[1] - expected) <= 0.01 * expected
+    assert abs(u[0]) < 1e-10 and abs(u[1]) < 1e-10
+
+
+@pytest.mark.parametrize("prec", [N.F64, N.F32])
+def test_corotating_and_leapfrog(ctx, prec):
+    d, G, s = 2.0, 1.0, 0.01
+    u, w = ctx.biot_savart_self([-d / 2, d / 2], [0, 0], [G, G], [s, s], prec)
+    e = G / (2 * math.pi * d)
+    assert abs(w[0] + e) <= 0.01 * e and abs(w[1] - e) <= 0.01 * e
+    # test_BiotSavart.cpp:117-161
+    x = [-1.0, -1.0, 1.0, 1.0]
+    z = [0.5, -0.5, 0.5, -0.5]
+    c = [1.0, -1.0, 1.0, -1.0]
+    u, w = ctx.biot_savart_self(x, z, c, [0.05] * 4, prec)
+    tol = 1e-10 if prec == N.F64 else 1e-6
+    assert np.all(np.isfinite(u)) and np.all(np.isfinite(w))
+    assert abs(u[0] - u[2]) < tol and abs(u[1] - u[3]) < tol
+
+
+def test_close_pair_finite(ctx):
+    # test_BiotSavart.cpp:89-114
+    for prec in (N.F64, N.F32):
+        u, w = ctx.biot_savart_self([-0.0005, 0.0005], [0, 0], [1, -1], [0.1, 0.1], prec)
+        assert np.all(np.isfinite(u)) and np.all(np.isfinite(w))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 255, 256, 257, 1023, 1024, 1025, 5000])
+def test_self_f64_vs_oracle(ctx, port, n):
+    x, z, g, s = W.wake(n, 10 + n, 0.0818804)
+    u0, w0 = port.direct_self(x, z, g, s)
+    u, w = ctx.biot_savart_self(x, z, g, s, N.F64)
+    scale = max(np.max(np.abs(u0)), np.max(np.abs(w0)), 1e-300)
+    assert np.max(np.abs(u - u0)) <= F64_TOL * scale
+    assert np.max(np.abs(w - w0)) <= F64_TOL * scale
+
+
+@pytest.mark.parametrize("n", [2, 100, 1024, 4097, 20000])
+def test_self_f32_vs_oracle(ctx, port, n):
+    x, z, g, s = W.wake(n, 20 + n, 0.0818804)
+    u0, w0 = port.direct_self(x, z, g, s)
+    u, w = ctx.biot_savart_self(x, z, g, s, N.F32)
+    assert rel_l2(u, u0) <= F32_REL_L2, rel_l2(u, u0)
+    assert rel_l2(w, w0) <= F32_REL_L2, rel_l2(w, w0)
+
+
+def test_self_f32_clustered_boundary_layer(ctx, port):
+    """Dense nascent-blob layer next to a body: close pairs dominate."""
+    rng = np.random.default_rng(3)
+    n = 8000
+    th = rng.uniform(0, 2 * np.pi, n)
+    r = 0.5 + np.abs(rng.normal(0, 0.01, n))
+    x, z = r * np.cos(th) + 3.0, r * np.sin(th) - 1.0
+    g = rng.normal(0, 1e-3, n)
+    s = np.full(n, 0.0818804)
+    u0, w0 = port.direct_self(x, z, g, s)
+    u, w = ctx.biot_savart_self(x, z, g, s, N.F32)
+    assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
+
+
+def test_coincident_distinct_blobs_match_reference_nan(ctx, port):
+    """Two distinct blobs at the same point: the reference divides 0/0 (NaN)."""
+    x, z = [0.0, 0.0, 1.0], [0.0, 0.0, 0.0]
+    u0, w0 = port.direct_self(x, z, [1.0, 1.0, 1.0], [0.1] * 3)
+    u, w = ctx.biot_savart_self(x, z, [1.0, 1.0, 1.0], [0.1] * 3, N.F64)
+    assert np.array_equal(np.isnan(u), np.isnan(u0))
+
+
+@pytest.mark.parametrize("prec", [N.F64, N.F32])
+def test_at_targets_vs_oracle(ctx, port, prec):
+    x, z, g, s = W.wake(6000, 5, 0.0818804)
+    tx, tz = W.collocation_circle(256)
+    tx = np.concatenate([tx, x[:10]])  # targets on blobs: r2 <= 1e-15 skipped (:89)
+    tz = np.concatenate([tz, z[:10]])
+    u0, w0 = port.direct_at(x, z, g, s, tx, tz)
+    u, w = ctx.biot_savart_at(x, z, g, s, tx, tz, prec)
+    if prec == N.F64:
+        sc = np.max(np.abs(u0)) + np.max(np.abs(w0))
+        assert np.max(np.abs(u - u0)) <= F64_TOL * sc and np.max(np.abs(w - w0)) <= F64_TOL * sc
+    else:
+        assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
+
+
+def test_at_single_target_known_answer(ctx):
+    # test_VelocityKernel.cpp:73-97
+    for prec in (N.F64, N.F32):
+        u, w = ctx.biot_savart_at([0.0], [0.0], [1.0], [0.1], [1.0], [0.0], prec)
+        assert abs(u[0]) < 1e-10
+        assert abs(w[0] - 1.0 / (2 * math.pi)) < 0.01
+
+
+def test_large_f32_properties(ctx):
+    """At 2^18 blobs (too big for the oracle here): antisymmetry of the pair
+    interaction gives sum_i Gamma_i u_i ~ 0 and w = 0 for a mirrored set."""
+    x, z, g, s = W.wake(1 << 18, 7, 0.0818804)
+    u, w = ctx.biot_savart_self(x, z, g, s, N.F32)
+    assert np.all(np.isfinite(u)) and np.all(np.isfinite(w))
+    # momentum-like invariant: sum Gamma_i * u_i is zero analytically
+    mom = abs(np.dot(g, u)) / (np.linalg.norm(g) * np.linalg.norm(u))
+    assert mom < 1e-5
+    # determinism: identical inputs give bit-identical outputs
+    u2, w2 = ctx.biot_savart_self(x, z, g, s, N.F32)
+    assert np.array_equal(u, u2) and np.array_equal(w, w2)
