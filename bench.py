@@ -1,0 +1,518 @@
+#!/usr/bin/env python
+"""Benchmark of the batched DVM step on B200.
+
+Workload ("batched", the metric's configuration): 64 independent bodies --
+circle R=0.5, ellipses of aspect U[1,4], rounded squares (side 1, corner
+radius 0.05) -- with panel counts log-uniform in [64, 512], each pre-seeded
+with a wake of log-uniform 1e4..4e5 blobs (seeded synthetic data), Euler,
+dt = 0.005, nu = 1e-3, ux = 1, REFLECT, FP32 compensated pair sums.
+
+A "step" advances all 64 simulations by one time step (DVMBase::compute_step
+each); value = simulation-steps per second over the whole job.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  Multi-GPU runs are replicas (each rank runs its own
+copy of the batch; no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched sim-steps/s vs plain GPU at <=1e-5 rel vel err; p50/p99 latency"
+UNIT = "sim-steps/s"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas: only timing values cross ranks)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = _env_int("WORLD_SIZE", 1)
+        self.rank = _env_int("RANK", 0)
+        self.local = _env_int("LOCAL_RANK", 0)
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="dvm_clocks_", suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                p = [q.strip() for q in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def make_instances(count: int, seed: int):
+    from dvmpp_b200 import workloads as W
+
+    return W.batched_instances(count, seed)
+
+
+def sim_params(inst, steps_total: int, prepush_steps: int):
+    from dvmpp_b200 import native as N
+
+    M = 3
+    grow = steps_total * (M + 1) * inst["npanels"] * 2  # release counts can exceed (M+1)
+    cap = inst["nblobs"] + grow
+    per_step = 2 * cap + 2 * (M + 1) * inst["npanels"]
+    return N.Params(rho=1.0, nu=1e-3, dt=0.005, ux=1.0, uz=0.0, cutoff_exp=0.675,
+                    max_numpanelvort=M, scheme=N.EULER, surface_cross=N.REFLECT,
+                    rng=N.RNG_INJECT, precision=N.F32, seed=1, capacity=cap,
+                    rng_capacity=prepush_steps * per_step + 1024)
+
+
+def pinned(n: int):
+    """A pinned host float64 buffer (torch allocates it; numpy views it)."""
+    import torch
+
+    return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+
+def uniforms_for(sims, rng, steps: int):
+    """(0,1] uniforms covering `steps` steps of every simulation."""
+    out = []
+    for s in sims:
+        n = s.n_hint
+        need = steps * (2 * n + 2 * (3 + 1) * s.np + 64)
+        out.append(1.0 - rng.random(need))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# the reference arm / CPU baseline: the reference's own code, phase-timed on
+# a sample of the instances and extrapolated by each phase's complexity
+# ---------------------------------------------------------------------------
+def _cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class RefModel:
+    """Per-phase cost rates of the reference step, fitted on sampled
+    instances: biotsavart ~ N^2, vortexsheetbc ~ N Np (serial in the
+    reference), rest of convect ~ N Np, diffusion + crossing ~ N,
+    release + loads ~ Np."""
+
+    def __init__(self):
+        self.acc = {"a": [], "b": [], "c": [], "d": [], "e": []}
+
+    def add(self, N, Np, t):
+        self.acc["a"].append(t["bs"] / max(N * N, 1))
+        self.acc["b"].append(t["sbc"] / max(N * Np, 1))
+        self.acc["c"].append(max(t["convect"] - t["bs"] - t["sbc"], 0.0) / max(N * Np, 1))
+        self.acc["d"].append((t["diff"] + t["cross"]) / max(N, 1))
+        self.acc["e"].append((t["rel"] + t["loads"]) / max(Np, 1))
+
+    def step_time(self, instances) -> float:
+        r = {k: float(np.mean(v)) for k, v in self.acc.items()}
+        tot = 0.0
+        for inst in instances:
+            N, Np = inst["nblobs"], inst["npanels"]
+            tot += r["a"] * N * N + (r["b"] + r["c"]) * N * Np + r["d"] * N + r["e"] * Np
+        return tot
+
+
+def ref_sample_step(ref, inst, workdir):
+    """One reference step (DVMBase::compute_step phases) on one instance, timed
+    per phase with the host clock (output writing is not part of it)."""
+    from oracle.pyoracle import SimParams
+
+    p = SimParams(rho=1.0, nu=1e-3, dt=0.005, ux=1.0, uz=0.0, cutoff_exp=0.675,
+                  max_numpanelvort=3, scheme="euler", surface_cross="REFLECT", seed=1, steps=10)
+    bx, bz = inst["body"]
+    s = ref.sim(p, bx, bz, workdir=workdir)
+    s.set_blobs(*inst["blobs"])
+    t = {}
+
+    def timed(key, phase):
+        t0 = time.perf_counter()
+        s.phase(phase)
+        t[key] = time.perf_counter() - t0
+
+    timed("bs", 0)
+    timed("sbc_solve", 1)
+    timed("sbc", 2)
+    timed("convect", 3)
+    timed("diff", 4)
+    timed("rel", 5)
+    timed("cross", 6)
+    timed("loads", 7)
+    # convect = biotsavart + solve + sheetbc + update; the separate bs/solve/sbc
+    # calls above measured its parts on the same state
+    t["convect"] = max(t["convect"], t["bs"] + t["sbc"])
+    del s
+    return t
+
+
+def reference_sample(instances, n_samples: int):
+    from oracle.pyoracle import Ref, have_ref
+
+    if not have_ref():
+        return None
+    ref = Ref()
+    order = sorted(range(len(instances)), key=lambda k: instances[k]["nblobs"])
+    pick = order[:n_samples]
+    model = RefModel()
+    total = 0.0
+    with tempfile.TemporaryDirectory(prefix="dvmref_") as wd:
+        for k in pick:
+            inst = instances[k]
+            t0 = time.perf_counter()
+            tt = ref_sample_step(ref, inst, wd)
+            total += time.perf_counter() - t0
+            model.add(inst["nblobs"], inst["npanels"], tt)
+    batch = model.step_time(instances)
+    return {"batch_step_s": batch, "sampled": [instances[k]["nblobs"] for k in pick],
+            "wall_s": total}
+
+
+def run_reference_arm(args, dist):
+    if dist.rank != 0:
+        return
+    instances = make_instances(args.instances, args.seed)
+    from oracle.pyoracle import have_ref
+
+    kind = "reference" if have_ref() else "port"
+    if kind != "reference":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libdvmref.so (the reference built from source) is absent"}))
+        return
+    os.environ.setdefault("OMP_NUM_THREADS", str(_cores()))
+    for _ in range(args.warmup):
+        reference_sample(instances, 1)
+    times = []
+    sampled = []
+    for k in range(args.steps):
+        r = reference_sample(instances, 1 + (k % 2))
+        times.append(r["batch_step_s"])
+        sampled.append(r["sampled"])
+    step_s = float(np.median(times))
+    value = args.instances / step_s
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "batched: 64 mixed bodies (circle / ellipse aspect U[1,4] / "
+                               "rounded square), panels log-U[64,512], wakes log-U[1e4,4e5] "
+                               "blobs, Euler dt=0.005, REFLECT", "instances": args.instances,
+                   "parallelism": "OpenMP host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": _cores(), "kind": kind,
+                         "sample": "each step: one reference DVMBase::compute_step, phase-timed, "
+                                   "on the 1-2 smallest instances; per-phase rates extrapolated "
+                                   "to all 64 instances by N^2, N*Np, N, Np"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def run_ours(args, dist):
+    from dvmpp_b200 import native as N
+
+    t_setup = time.perf_counter()
+    instances = make_instances(args.instances, args.seed)
+    ctx = N.Context(dist.local)
+    sms, ccmaj, ccmin = ctx.device_info()
+    steps_total = args.warmup + args.steps + args.prof_steps + args.plain_steps + args.e2e_steps + 2
+    prepush = args.warmup + args.steps + args.prof_steps + args.plain_steps + 1
+    sims = []
+    for inst in instances:
+        p = sim_params(inst, steps_total, prepush)
+        bx, bz = inst["body"]
+        s = ctx.sim(p, bx, bz)
+        s.set_blobs(*inst["blobs"])
+        s.n_hint = p.capacity
+        sims.append(s)
+    rng = np.random.default_rng(1234 + dist.rank)
+    for s, u in zip(sims, uniforms_for(sims, rng, prepush)):
+        s.push_uniforms(u)
+    setup_s = time.perf_counter() - t_setup
+
+    # warm-up (first step eager, then graph captured and replayed)
+    ctx.step_batch(sims, args.warmup, use_graph=True)
+    for s in sims:
+        s.check()
+    ctx.sync()
+
+    # ---- timed region: K batched steps, inputs resident in HBM, graph replay
+    clocks = ClockSampler(dist.local)
+    dist.barrier()
+    ctx.sync()
+    clocks.start()
+    l0 = ctx.launches()
+    ctx.mark(0)
+    ctx.step_batch(sims, args.steps, use_graph=True)
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    launches = ctx.launches() - l0
+    clock_info = clocks.stop()
+    for s in sims:
+        s.check()
+    ms_max = dist.max(ms)
+    value = dist.world * args.instances * args.steps / (ms_max / 1e3)
+
+    # ---- profiled steps (eager, CUDA events around every kernel family)
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    pairs = 0
+    for _ in range(args.prof_steps):
+        ns = [s.n for s in sims]
+        pairs += sum(n * (n - 1) for n in ns)
+        ctx.step_batch(sims, 1, use_graph=False)
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    nb_ms, nb_n = prof["nbody"]
+    step_ms_prof = prof["step"][0] / max(prof["step"][1], 1)
+    nbody_launch_ms = nb_ms / max(nb_n, 1)
+    pairs_per_launch = pairs / max(nb_n, 1)
+    achieved_tflops = 12.0 * pairs_per_launch / (nbody_launch_ms / 1e3) / 1e12
+    pk = peaks()
+    sm_max = float(pk.get("sm_max_mhz", 1965.0))
+    fp32_peak = sms * 128 * 2 * sm_max * 1e6 / 1e12
+
+    # ---- plain GPU path: one simulation at a time, same kernels, no batching
+    ctx.sync()
+    ctx.mark(2)
+    for _ in range(args.plain_steps):
+        for s in sims:
+            s.step(1)
+    ctx.mark(3)
+    plain_ms = ctx.elapsed_ms(2, 3)
+    for s in sims:
+        s.check()
+    plain_ms = dist.max(plain_ms)
+    plain_value = dist.world * args.instances * args.plain_steps / (plain_ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        hbuf = [pinned(max(2 * s.n_hint + 8 * s.np + 64, 1)) for s in sims]
+        out_x = [pinned(s.n_hint) for s in sims]
+        out_z = [pinned(s.n_hint) for s in sims]
+        out_c = [pinned(s.n_hint) for s in sims]
+        h2d = d2h = 0
+        dist.barrier()
+        ctx.sync()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            for s, hb in zip(sims, hbuf):
+                n = s.n  # blob count before the step
+                need = 2 * n + 2 * (3 + 1) * s.np + 64
+                hb[:need] = 1.0 - rng.random(need)
+                s.push_uniforms(hb[:need])
+                h2d += need * 8
+            ctx.step_batch(sims, 1, use_graph=True)
+            for s, ox, oz, oc in zip(sims, out_x, out_z, out_c):
+                s.get_state_into(ox, oz, oc)
+                s.loads()
+                d2h += 3 * 8 * s.last_n + 4 * 8
+        ctx.sync()
+        e2e_s = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.world * args.instances * args.e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d / args.e2e_steps),
+               "d2h_bytes_per_step": int(d2h / args.e2e_steps),
+               "note": "per step: uniforms pushed (inject mode) from pinned host memory, one "
+                       "batched step, x/z/circ of every blob and the loads read back "
+                       "(what DVMBase::write_outputs consumes); host wall clock"}
+        for s in sims:
+            s.check()
+
+    # ---- CPU baseline (rank 0, N = 1): the reference itself, bounded sample
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        r = reference_sample(instances, 2)
+        if r:
+            cpu = {"value": args.instances / r["batch_step_s"], "unit": UNIT, "cores": _cores(),
+                   "kind": "reference",
+                   "sample": f"one reference compute_step (phase-timed) on each of the 2 "
+                             f"smallest instances (N={r['sampled']}), per-phase rates "
+                             f"extrapolated to all {args.instances} instances; output writing "
+                             f"off; {r['wall_s']:.1f} s of CPU work"}
+
+    nblobs = [s.n for s in sims]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 pair sums (Kahan), f64 state/sheet",
+        "data": "synthetic (seeded bodies and wakes)",
+        "config": {"workload": "batched: 64 mixed bodies (circle / ellipse aspect U[1,4] / "
+                               "rounded square), panels log-U[64,512], wakes log-U[1e4,4e5] "
+                               "blobs, Euler dt=0.005, nu=1e-3, ux=1, REFLECT, FP32 compensated",
+                   "instances": args.instances, "blobs_total": int(sum(nblobs)),
+                   "panels_total": int(sum(s.np for s in sims)),
+                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (state + workspace >> 126 MB)",
+                   "graph": "one CUDA graph per step, replayed"},
+        "plain_gpu": {"value": plain_value, "unit": UNIT, "steps": args.plain_steps,
+                      "ratio_batched_over_plain": value / plain_value,
+                      "how": "each simulation stepped alone (its own launches, no batching)"},
+        "roofline": {"bound": "fp32", "kernel": "k_self_f32 (pair kernel)",
+                     "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved_tflops / fp32_peak, "traffic": args.traffic,
+                     "flops_per_pair": 12, "pairs_per_launch": pairs_per_launch,
+                     "launch_ms": nbody_launch_ms,
+                     "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 x "
+                                    f"{sm_max:.0f} MHz (sm_max_mhz of MEASURED_PEAKS.json); "
+                                    f"that file has no FP32 figure",
+                     "share_of_step": nb_ms / max(prof["step"][0], 1e-9)},
+        "profile_ms_per_step": {k: v[0] / max(args.prof_steps, 1) for k, v in prof.items()},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+        "setup_s": setup_s,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if cpu:
+        line["cpu_baseline"] = cpu
+    if dist.rank == 0:
+        print(json.dumps(line))
+    for s in sims:
+        s.close()
+    ctx.close()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--prof-steps", type=int, default=2)
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--traffic", type=float, default=None,
+                    help="dram bytes per pair-kernel launch from an ncu capture")
+    args = ap.parse_args(argv)
+    args.warmup = max(args.warmup, 3)
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, dist)
+        else:
+            run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

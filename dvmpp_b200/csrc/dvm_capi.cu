@@ -102,6 +102,7 @@ struct dvm_ctx {
     std::vector<cudaEvent_t> pool;
     double prof_ms[DVM_PROF_FAMILIES] = {};
     uint64_t prof_n[DVM_PROF_FAMILIES] = {};
+    cudaEvent_t marks[16] = {};
 };
 
 struct dvm_sim {
@@ -565,6 +566,8 @@ int dvm_ctx_destroy(dvm_ctx* c) {
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->marks)
+        if (e) cudaEventDestroy(e);
     if (c->ws_block) cudaFree(c->ws_block);
     if (c->raw_block) cudaFree(c->raw_block);
     if (c->d_table) cudaFree(c->d_table);
@@ -592,6 +595,23 @@ int dvm_ctx_device_info(dvm_ctx* c, int* sms, int* ma, int* mi) {
     if (sms) *sms = c->sms;
     if (ma) *ma = c->cc_major;
     if (mi) *mi = c->cc_minor;
+    return DVM_OK;
+}
+
+int dvm_ctx_mark(dvm_ctx* c, int slot) {
+    if (!c || slot < 0 || slot >= 16) return fail(DVM_ERR_ARG, "bad marker slot");
+    if (!c->marks[slot]) CK(cudaEventCreate(&c->marks[slot]));
+    CK(cudaEventRecord(c->marks[slot], c->stream));
+    return DVM_OK;
+}
+
+int dvm_ctx_elapsed(dvm_ctx* c, int a, int b, double* ms) {
+    if (!c || !ms || a < 0 || a >= 16 || b < 0 || b >= 16 || !c->marks[a] || !c->marks[b])
+        return fail(DVM_ERR_ARG, "bad marker slot");
+    CK(cudaEventSynchronize(c->marks[b]));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, c->marks[a], c->marks[b]));
+    *ms = f;
     return DVM_OK;
 }
 
@@ -1024,7 +1044,18 @@ int dvm_sim_phase(dvm_sim* s, int phase) {
     const ListEntry* L = pl->all.d_list;
     const int np = s->h.np, prec = s->h.precision;
     switch (phase) {
-        case DVM_PHASE_BIOTSAVART: biot_savart_self(T, S, L, 1, prec, ws, c->sms, st); break;
+        case DVM_PHASE_BIOTSAVART: {
+            int pr = prof_begin(c, DVM_PROF_SORT);
+            biot_savart_prepare(T, S, L, 1, prec, ws, c->sms, st);
+            prof_end(c, pr);
+            pr = prof_begin(c, DVM_PROF_NBODY);
+            biot_savart_compute(T, S, L, 1, prec, ws, c->sms, st);
+            prof_end(c, pr);
+            pr = prof_begin(c, DVM_PROF_SORT);
+            biot_savart_finish(T, S, L, 1, prec, ws, c->sms, st);
+            prof_end(c, pr);
+            break;
+        }
         case DVM_PHASE_SOLVE:
             sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
             sheet_solve(T, S, L, 1, np, st);

@@ -66,6 +66,8 @@ SIGNATURES = {
     "dvm_ctx_device_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "dvm_ctx_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "dvm_sim_bytes": (C.c_int, [C.POINTER(SimParams), C.c_int, C.POINTER(C.c_uint64)]),
+    "dvm_ctx_mark": (C.c_int, [C.c_void_p, C.c_int]),
+    "dvm_ctx_elapsed": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     "dvm_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "dvm_ctx_profile": (C.c_int, [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_uint64)]),
     "dvm_ctx_profile_reset": (C.c_int, [C.c_void_p]),
@@ -164,6 +166,14 @@ class Context:
         s, ma, mi = C.c_int(), C.c_int(), C.c_int()
         _check(self.lib.dvm_ctx_device_info(self.h, C.byref(s), C.byref(ma), C.byref(mi)))
         return s.value, ma.value, mi.value
+
+    def mark(self, slot: int):
+        _check(self.lib.dvm_ctx_mark(self.h, slot))
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        v = C.c_double()
+        _check(self.lib.dvm_ctx_elapsed(self.h, a, b, C.byref(v)))
+        return v.value
 
     def set_profiling(self, on: bool):
         _check(self.lib.dvm_ctx_set_profiling(self.h, 1 if on else 0))
@@ -291,6 +301,16 @@ class Simulation:
         d = dict(zip(["x", "z", "circ", "sigma", "u", "w", "uvs", "wvs"], arrs))
         d["id"] = ids
         return d
+
+    def get_state_into(self, x, z, circ):
+        """Copy positions and circulations into caller buffers (e.g. pinned);
+        returns the blob count (also kept in self.last_n)."""
+        nn = C.c_uint64()
+        cap = min(x.size, z.size, circ.size)
+        _check(self.lib.dvm_sim_get_blobs(self.h, cap, C.byref(nn), _p(x), _p(z), _p(circ),
+                                          None, None, None, None, None, None))
+        self.last_n = nn.value
+        return nn.value
 
     def gamma(self):
         g = np.empty(self.np)

@@ -138,6 +138,11 @@ int dvm_ctx_launch_count(dvm_ctx* ctx, uint64_t* launches);
 #define DVM_PROF_SORT 7       /* Morton sort, pack, partial combine */
 #define DVM_PROF_STEP 8       /* whole step */
 #define DVM_PROF_FAMILIES 9
+/* Timing markers: dvm_ctx_mark records CUDA event `slot` (0..15) on the ctx
+ * stream; dvm_ctx_elapsed synchronises and returns the device time between
+ * two recorded markers. */
+int dvm_ctx_mark(dvm_ctx* ctx, int slot);
+int dvm_ctx_elapsed(dvm_ctx* ctx, int slot_a, int slot_b, double* ms);
 int dvm_ctx_set_profiling(dvm_ctx* ctx, int on);
 int dvm_ctx_profile(dvm_ctx* ctx, int family, double* ms_total, uint64_t* launches);
 int dvm_ctx_profile_reset(dvm_ctx* ctx);
