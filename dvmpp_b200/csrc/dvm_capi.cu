@@ -31,6 +31,13 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+// Lets entry points defined in other translation units set dvm_last_error().
+int dvmk::report_error(int code, const char* msg) { return fail(code, msg); }
+
+namespace {
+
 #define CK(call)                                                                          \
     do {                                                                                  \
         cudaError_t e_ = (call);                                                          \

@@ -147,6 +147,9 @@ struct Workspace {
     int key_bits = 40;
 };
 
+// Sets the calling thread's dvm_last_error() message; returns `code`.
+int report_error(int code, const char* msg);
+
 // ---- launchers (all asynchronous on `s`) ------------------------------------
 size_t cub_sort_bytes(uint64_t total);
 

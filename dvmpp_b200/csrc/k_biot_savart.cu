@@ -21,6 +21,9 @@
 // FP64 path (the parity path): same work decomposition in original blob order
 // and the reference's exact operation sequence (no FMA contraction).
 #include <cfloat>
+#include <mutex>
+#include <string>
+
 #include <cub/cub.cuh>
 
 #include "dvm_device.cuh"
@@ -701,4 +704,103 @@ void direct_at_raw(const double* x, const double* z, const double* circ, const d
     }
 }
 
+// ---- at-target velocity with fixed, library-owned scratch -------------------
+// For callers that must not allocate device memory (see
+// dvm_biot_savart_at_noalloc in include/dvm_cuda.h).  The chunk partials of
+// k_at live in this file-scope array instead of a caller- or context-owned
+// buffer; every GPU that loads the library holds it until the process exits.
+namespace {
+
+constexpr size_t kNoAllocElems = 262144;  // double2 entries: 4 MiB per device
+constexpr size_t kNoAllocJobElems = 64;   // tail entries that hold the job record
+static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocElems];
+
+struct NoAllocDevice {
+    double2* scratch = nullptr;  // device address of g_noalloc_scratch
+    int sms = 0;
+    bool ready = false;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+__global__ void k_write_job(AtJob* dst, AtJob job) { *dst = job; }
+
+}  // namespace
+
 }  // namespace dvmk
+
+extern "C" int dvm_biot_savart_at_noalloc(const double* x, const double* z, const double* circ,
+                                          const double* sigma, uint64_t ns, const double* tx,
+                                          const double* tz, uint64_t nt, double* u, double* w,
+                                          int precision, int skip_close, void* stream) {
+    using namespace dvmk;
+    if (nt && (!tx || !tz || !u || !w)) return report_error(1, "null target or output array");
+    if (ns && (!x || !z || !circ || !sigma)) return report_error(1, "null source array");
+    if (precision != kF64 && precision != kF32) return report_error(1, "bad precision");
+    if (nt == 0) return 0;
+    const size_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    const size_t npad = std::max<size_t>((nt + 255) / 256 * 256, 256);
+    if (ns > 0xF0000000ull || nt > 0xF0000000ull ||
+        nchunk * npad > kNoAllocElems - kNoAllocJobElems) {
+        return report_error(
+            1, "dvm_biot_savart_at_noalloc: ceil(ns/4096) * ceil(nt/256) * 256 must not exceed "
+               "262080 (fixed 4 MiB scratch); use dvm_biot_savart_at_device for larger sizes");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+        return report_error(3, "dvm_biot_savart_at_noalloc: no current CUDA device");
+    NoAllocDevice& D = g_noalloc_dev[dev];
+    {
+        // One-time set-up per device, with that device current: the address of
+        // the file-scope array (host code cannot use the symbol itself).
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!D.ready) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return report_error(3, (std::string("cudaGetSymbolAddress: ") +
+                                        cudaGetErrorString(e)).c_str());
+            int sms = 0;
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            if (e != cudaSuccess)
+                return report_error(3, (std::string("cudaDeviceGetAttribute: ") +
+                                        cudaGetErrorString(e)).c_str());
+            D.scratch = static_cast<double2*>(p);
+            D.sms = sms;
+            D.ready = true;
+        }
+    }
+    if (ns == 0) {  // no sources: zero velocity, as the reference's empty loop gives
+        if (cudaMemsetAsync(u, 0, sizeof(double) * nt, s) != cudaSuccess ||
+            cudaMemsetAsync(w, 0, sizeof(double) * nt, s) != cudaSuccess)
+            return report_error(3, "cudaMemsetAsync failed");
+        return 0;
+    }
+    AtJob J;
+    J.tx = tx;
+    J.tz = tz;
+    J.nt = (uint32_t)nt;
+    J.skip_close = skip_close ? 1 : 0;
+    J.sx = x;
+    J.sz = z;
+    J.sc = circ;
+    J.ss = sigma;
+    J.pns = nullptr;
+    J.ns = (uint32_t)ns;
+    J.npad = (int)npad;
+    J.part = D.scratch;  // every entry read by k_at_combine is written by k_at first
+    J.circ_part = nullptr;
+    AtJob* job = reinterpret_cast<AtJob*>(D.scratch + (kNoAllocElems - kNoAllocJobElems));
+    k_write_job<<<1, 1, 0, s>>>(job, J);
+    if (precision == kF32) k_at<true><<<D.sms * 4, 256, 0, s>>>(job, 1);
+    else k_at<false><<<D.sms * 4, 256, 0, s>>>(job, 1);
+    const unsigned cb = (unsigned)std::min<uint64_t>((nt + 255) / 256, (uint64_t)D.sms * 8);
+    k_at_combine<<<std::max(1u, cb), 256, 0, s>>>(job, u, w);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return report_error(3, (std::string("dvm_biot_savart_at_noalloc launch: ") +
+                                cudaGetErrorString(e)).c_str());
+    return 0;
+}

@@ -77,6 +77,8 @@ SIGNATURES = {
     "dvm_biot_savart_self_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int]),
     "dvm_biot_savart_at_device": (C.c_int, [C.c_void_p] + [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2
                                   + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int, C.c_int]),
+    "dvm_biot_savart_at_noalloc": (C.c_int, [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2
+                                   + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int, C.c_int, C.c_void_p]),
     "dvm_sim_create": (C.c_int, [C.c_void_p, C.POINTER(SimParams), _dp, _dp, C.c_int, C.POINTER(C.c_void_p)]),
     "dvm_sim_destroy": (C.c_int, [C.c_void_p]),
     "dvm_sim_set_blobs": (C.c_int, [C.c_void_p, C.c_uint64, _dp, _dp, _dp, _dp]),

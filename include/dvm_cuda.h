@@ -164,6 +164,30 @@ int dvm_biot_savart_at_device(dvm_ctx* ctx, const double* x, const double* z, co
                               const double* tz, uint64_t nt, double* u, double* w,
                               int precision, int skip_close);
 
+/* Velocity at targets without any device allocation.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc: code whose device memory is owned by a host framework's
+ * allocator or memory pool (a stray allocation would fail or fragment it),
+ * plug-in hosts that forbid allocation outside their own allocator, and
+ * latency-critical loops that cannot afford an allocation's implicit
+ * synchronisation.  It needs no dvm_ctx.  The caller passes device buffers
+ * for inputs and outputs; the chunk partials live in a fixed 4 MiB array
+ * inside the library, which every GPU that loads the library keeps until the
+ * process exits.  Limit: ceil(ns/4096) * ceil(nt/256) * 256 <= 262080 (for
+ * example ns up to 1,048,576 sources with nt up to 256 targets); larger sizes
+ * are rejected with DVM_ERR_ARG.  The first call on a device looks up that
+ * array's device address (with the device current), so make it before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (different streams, or different host threads) race and corrupt each
+ * other's results; serialise them on one stream.  Nothing needs clearing
+ * between calls: every partial is written before it is read.  Asynchronous on
+ * `stream` (a cudaStream_t, or NULL for the default stream).  Arguments and
+ * results are those of dvm_biot_savart_at_device. */
+int dvm_biot_savart_at_noalloc(const double* x, const double* z, const double* circ,
+                               const double* sigma, uint64_t ns, const double* tx,
+                               const double* tz, uint64_t nt, double* u, double* w,
+                               int precision, int skip_close, void* stream);
+
 /* ---- simulations ---------------------------------------------------------------- */
 /* body_x/body_z: closed CCW contour of npoints (first point repeated last),
  * the reference's domain_file format (src/VortexSheet.cpp:56-76). */
