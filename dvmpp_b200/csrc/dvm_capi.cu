@@ -49,9 +49,16 @@ constexpr int kTableCap = 4096;
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Source chunks of a simulation's pair kernel.  Fixed by the capacity alone, so
+// a simulation's sums are associated the same way alone and inside any batch:
+// at least one chunk per 64 k sources, and for small simulations enough chunks
+// (>= ~2^21 / cap items per 256-target tile) to occupy the GPU when stepped
+// alone, but never chunks shorter than 8 k sources.
 int nbody_chunks(uint32_t cap) {
-    const int c = (int)((cap + 65535) / 65536);
-    return std::max(1, std::min(16, c));
+    const int by_size = (int)((cap + 65535) / 65536);
+    const int by_fill = (int)((2u << 20) / std::max<uint32_t>(cap, 1));
+    const int most = (int)std::max<uint32_t>(1, std::min<uint32_t>(64, cap / 8192));
+    return std::max(1, std::min(most, std::max(by_size, by_fill)));
 }
 
 }  // namespace
@@ -234,6 +241,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     w.vals_in = reinterpret_cast<uint32_t*>(b + o_vals);
     w.perm = reinterpret_cast<uint32_t*>(b + o_perm);
     w.packed = reinterpret_cast<double4*>(b + o_packed);
+    w.packed_cap = cap;
     w.meta = reinterpret_cast<TileMeta*>(b + o_meta);
     w.part = reinterpret_cast<double2*>(b + o_part);
     w.rhs_part = reinterpret_cast<double2*>(b + o_rhs);

@@ -132,7 +132,9 @@ struct Workspace {
     uint64_t* keys_out = nullptr;
     uint32_t* vals_in = nullptr;
     uint32_t* perm = nullptr;      // sorted slot -> original blob index
-    double4* packed = nullptr;     // sorted (x, z, circ, sigma)
+    double4* packed = nullptr;     // sorted (x, z, circ, sigma); the FP32 path reuses it as
+                                   // double2 (x, z) | float4 (circ, 10 sigma^2, 1/sigma^2, -)
+    uint64_t packed_cap = 0;       // slots of `packed`
     TileMeta* meta = nullptr;      // total_cap / kBsST
     double2* part = nullptr;       // N-body partials
     double2* rhs_part = nullptr;   // at-target partials

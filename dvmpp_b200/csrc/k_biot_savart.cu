@@ -86,6 +86,8 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
                                                 const ListEntry* __restrict__ list, int nlist,
                                                 const uint32_t* __restrict__ perm,
                                                 double4* __restrict__ packed,
+                                                double2* __restrict__ pxz,
+                                                float4* __restrict__ pf,
                                                 TileMeta* __restrict__ meta) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ double s_red[5][kBsST / 32];
@@ -109,7 +111,13 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
         if (i < n) {
             const uint32_t p = perm ? perm[e.coff + i] : i;
             const double4 v = make_double4(d.x[p], d.z[p], d.circ[p], d.sigma[p]);
-            packed[e.coff + i] = v;
+            if (pxz) {  // FP32 path: positions in FP64, per-source constants in FP32
+                const double s2 = v.w * v.w;
+                pxz[e.coff + i] = make_double2(v.x, v.y);
+                pf[e.coff + i] = make_float4((float)v.z, (float)(10.0 * s2), (float)(1.0 / s2), 0.f);
+            } else {
+                packed[e.coff + i] = v;
+            }
             xmin = xmax = v.x;
             zmin = zmax = v.y;
             thr = 10.0 * (v.w * v.w);
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
     }
 }
 
-__device__ __forceinline__ void item_prefix_self(unsigned* s_pre, const InstState* st,
+__device__ __forceinline__ void item_prefix_f64(unsigned* s_pre, const InstState* st,
                                                  const ListEntry* list, int nlist) {
     if (threadIdx.x == 0) {
         unsigned acc = 0;
@@ -171,148 +179,280 @@ __device__ __forceinline__ uint32_t chunk_size(uint32_t n, int chunks) {
 }
 
 // ---- FP32 pair loops --------------------------------------------------------
-__device__ __forceinline__ void stage_far(const float4* __restrict__ src, const float (&tx)[kBsR],
-                                          const float (&tz)[kBsR], float (&pu)[kBsR],
-                                          float (&pw)[kBsR]) {
-#pragma unroll 8
+// A work item belongs to ONE warp: 256 consecutive sorted targets (8 per lane)
+// against one source chunk.  The warp stages its own source tiles in shared
+// memory and never waits for other warps, so far-path and near-path warps of a
+// block do not hold each other up at barriers.
+constexpr int kWR = 8;                // consecutive targets per lane
+constexpr int kWP = kWR / 2;          // target pairs per lane (packed FP32x2)
+constexpr int kWTT = 32 * kWR;        // targets per warp item
+constexpr int kWWarps = 4;            // independent warps per block
+#ifndef DVM_SELF_MINBLOCKS
+#define DVM_SELF_MINBLOCKS 3          // blocks per SM the register budget is sized for
+#endif
+
+// Packed FP32x2 arithmetic (sm_100): one instruction operates on a pair of
+// targets, halving the issue slots of the pair loop; each half is rounded
+// exactly like the scalar instruction (round-to-nearest).
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float f2lo(uint64_t v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return lo;
+}
+__device__ __forceinline__ float f2hi(uint64_t v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return hi;
+}
+__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// Staged source: A = (x, x, z, z), B = (Gamma, Gamma, 10 sigma^2, 1/sigma^2), so
+// the far loop loads the duplicated pairs straight into 64-bit registers.
+struct StagedSrc {
+    float4 a;
+    float4 b;
+};
+
+// Target pairs (of kWP per lane) whose two reciprocals share one MUFU.RCP.
+#ifndef DVM_PAIR_RCP
+#define DVM_PAIR_RCP 0
+#endif
+constexpr int kPairRcp = DVM_PAIR_RCP;
+#ifndef DVM_FAR_UNROLL
+#define DVM_FAR_UNROLL 8
+#endif
+constexpr int kFarUnroll = DVM_FAR_UNROLL;  // sources per unrolled far-loop body
+
+// Far pairs: no core test.  Accumulates -u (so every update is one FMA) and w.
+__device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
+                                          const uint64_t (&tx2)[kWP], const uint64_t (&tz2)[kWP],
+                                          uint64_t (&nu2)[kWP], uint64_t (&w2)[kWP]) {
+#pragma unroll kFarUnroll
     for (int jj = 0; jj < kBsST; ++jj) {
-        const float4 s = src[jj];
+        const float4 A = src[jj].a;
+        const float4 B = src[jj].b;
+        const uint64_t sx = f2pack(A.x, A.y), sz = f2pack(A.z, A.w), sg = f2pack(B.x, B.y);
 #pragma unroll
-        for (int r = 0; r < kBsR; ++r) {
-            const float dx = tx[r] - s.x;
-            const float dz = tz[r] - s.y;
-            const float r2 = fmaf(dx, dx, dz * dz);
-            const float g = rcp_approx(r2) * s.z;
-            pu[r] = fmaf(-g, dz, pu[r]);
-            pw[r] = fmaf(g, dx, pw[r]);
+        for (int q = 0; q < kWP; ++q) {
+            const uint64_t dx = f2sub(tx2[q], sx);
+            const uint64_t dz = f2sub(tz2[q], sz);
+            const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
+            uint64_t inv;
+            if (q < kPairRcp) {
+                // one MUFU for both halves: 1/(a b) * b = 1/a, 1/(a b) * a = 1/b.
+                // Far pairs have 10 sigma^2 <= r2 <~ 1e4 (item-relative), so a*b
+                // stays normal; padded sources give rcp(inf) = 0 and Gamma = 0.
+                const float a = f2lo(r2), b = f2hi(r2);
+                const float ip = rcp_approx(a * b);
+                inv = f2pack(b * ip, a * ip);
+            } else {
+                inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
+            }
+            const uint64_t g = f2mul(inv, sg);
+            nu2[q] = f2fma(g, dz, nu2[q]);
+            w2[q] = f2fma(g, dx, w2[q]);
         }
     }
 }
 
-__device__ __forceinline__ void stage_near(const float4* __restrict__ src,
-                                           const float* __restrict__ rs,
-                                           const float (&tx)[kBsR], const float (&tz)[kBsR],
-                                           float (&pu)[kBsR], float (&pw)[kBsR], int tbase,
-                                           int jbase) {
-#pragma unroll 2
-    for (int jj = 0; jj < kBsST; ++jj) {
-        const float4 s = src[jj];
+// Core kernel (1 - exp(-r2/sigma^2)) / r2 in FP32.  expm1 keeps close pairs
+// accurate; below FLT_MIN the r -> 0 limit 1/sigma^2 is used.  That limit
+// covers the self pair (dx = dz = 0, so its contribution is exactly zero, as
+// the reference's i != j skip gives) and distinct blobs closer than FP32 can
+// resolve (nascent blobs of one panel can be), where the FP64 reference is
+// finite too.
+__device__ __forceinline__ float core_kernel(float r2, float rs, float rcp_r2) {
+    const float e = expm1f(-r2 * rs);
+    return r2 > 1e-30f ? -e * rcp_r2 : rs;
+}
+
+// Near pairs: the reference's exact test per pair (scalar; rare).
+__device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
+                                           const uint64_t (&tx2)[kWP], const uint64_t (&tz2)[kWP],
+                                           uint64_t (&nu2)[kWP], uint64_t (&w2)[kWP]) {
+    float nu[kWR], w[kWR], tx[kWR], tz[kWR];
 #pragma unroll
-        for (int r = 0; r < kBsR; ++r) {
-            const float dx = tx[r] - s.x;
-            const float dz = tz[r] - s.y;
+    for (int q = 0; q < kWP; ++q) {
+        tx[2 * q] = f2lo(tx2[q]);
+        tx[2 * q + 1] = f2hi(tx2[q]);
+        tz[2 * q] = f2lo(tz2[q]);
+        tz[2 * q + 1] = f2hi(tz2[q]);
+        nu[2 * q] = f2lo(nu2[q]);
+        nu[2 * q + 1] = f2hi(nu2[q]);
+        w[2 * q] = f2lo(w2[q]);
+        w[2 * q + 1] = f2hi(w2[q]);
+    }
+#pragma unroll 1
+    for (int jj = 0; jj < kBsST; ++jj) {
+        const float4 A = src[jj].a;
+        const float4 B = src[jj].b;
+#pragma unroll
+        for (int r = 0; r < kWR; ++r) {
+            const float dx = tx[r] - A.x;
+            const float dz = tz[r] - A.z;
             const float r2 = fmaf(dx, dx, dz * dz);
             float K = rcp_approx(r2);
-            if (r2 < s.w) {
-                // 1 - exp(-r2/sigma^2) through expm1 keeps close pairs accurate.
-                const float e = expm1f(-r2 * rs[jj]);
-                K = (tbase + r == jbase + jj) ? 0.0f : -e * K;
-            }
-            const float g = K * s.z;
-            pu[r] = fmaf(-g, dz, pu[r]);
-            pw[r] = fmaf(g, dx, pw[r]);
+            if (r2 < B.z) K = core_kernel(r2, B.w, K);
+            const float g = K * B.x;
+            nu[r] = fmaf(g, dz, nu[r]);
+            w[r] = fmaf(g, dx, w[r]);
         }
+    }
+#pragma unroll
+    for (int q = 0; q < kWP; ++q) {
+        nu2[q] = f2pack(nu[2 * q], nu[2 * q + 1]);
+        w2[q] = f2pack(w[2 * q], w[2 * q + 1]);
     }
 }
 
-__global__ void __launch_bounds__(kBsThreads, 2)
+__device__ __forceinline__ void kahan(float& s, float& c, float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+__global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
     k_self_f32(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
-               const double4* __restrict__ packed, const TileMeta* __restrict__ meta,
-               double2* __restrict__ part, unsigned* __restrict__ work) {
+               const double2* __restrict__ pxz, const float4* __restrict__ pf,
+               const TileMeta* __restrict__ meta, double2* __restrict__ part,
+               unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
-    __shared__ float4 s_src[kBsST];
-    __shared__ float s_rs[kBsST];
-    __shared__ unsigned s_item;
-    item_prefix_self(s_pre, st, list, nlist);
+    __shared__ StagedSrc s_src[kWWarps][kBsST];
+    __shared__ double s_box[kWWarps][4];
+    if (threadIdx.x == 0) {
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            acc += ((st[list[k].inst].n + kWTT - 1) / kWTT) * (unsigned)list[k].chunks;
+        }
+        s_pre[nlist] = acc;
+    }
+    __syncthreads();
     const unsigned total = s_pre[nlist];
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    StagedSrc* __restrict__ wsrc = s_src[wid];
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(work, 1u);
-        __syncthreads();
-        const unsigned item = s_item;
-        __syncthreads();
+        unsigned item = 0;
+        if (lane == 0) item = atomicAdd(work, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= total) break;
         const int k = locate(s_pre, nlist, item);
         const ListEntry e = list[k];
         const uint32_t n = st[e.inst].n;
         const unsigned local = item - s_pre[k];
         const uint32_t tile = local / e.chunks, c = local % e.chunks;
-        const uint32_t t0 = tile * kBsTT;
+        const uint32_t t0 = tile * kWTT;
         const uint32_t cs = chunk_size(n, e.chunks);
         const uint32_t j0 = c * cs, j1 = min(n, j0 + cs);
-        const double4* __restrict__ P = packed + e.coff;
-        const double ox = P[t0].x, oz = P[t0].y;
+        const double2* __restrict__ X = pxz + e.coff;
+        const float4* __restrict__ F = pf + e.coff;
+        const double2 o = X[t0];  // the item's origin: its first target
 
-        float tx[kBsR], tz[kBsR];
+        uint64_t tx2[kWP], tz2[kWP];
         double wxmin = DBL_MAX, wxmax = -DBL_MAX, wzmin = DBL_MAX, wzmax = -DBL_MAX;
-        const uint32_t tb = t0 + tid * kBsR;
+        const uint32_t tb = t0 + lane * kWR;
 #pragma unroll
-        for (int r = 0; r < kBsR; ++r) {
-            tx[r] = 0.0f;
-            tz[r] = 0.0f;
-            if (tb + r < n) {
-                const double4 p = P[tb + r];
-                tx[r] = (float)(p.x - ox);
-                tz[r] = (float)(p.y - oz);
-                wxmin = fmin(wxmin, p.x);
-                wxmax = fmax(wxmax, p.x);
-                wzmin = fmin(wzmin, p.y);
-                wzmax = fmax(wzmax, p.y);
+        for (int q = 0; q < kWP; ++q) {
+            float xs[2], zs[2];
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                xs[h] = 0.0f;
+                zs[h] = 0.0f;
+                const uint32_t t = tb + 2 * q + h;
+                if (t < n) {
+                    const double2 p = X[t];
+                    xs[h] = (float)(p.x - o.x);
+                    zs[h] = (float)(p.y - o.y);
+                    wxmin = fmin(wxmin, p.x);
+                    wxmax = fmax(wxmax, p.x);
+                    wzmin = fmin(wzmin, p.y);
+                    wzmax = fmax(wzmax, p.y);
+                }
             }
+            tx2[q] = f2pack(xs[0], xs[1]);
+            tz2[q] = f2pack(zs[0], zs[1]);
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            wxmin = fmin(wxmin, __shfl_xor_sync(0xffffffffu, wxmin, o));
-            wxmax = fmax(wxmax, __shfl_xor_sync(0xffffffffu, wxmax, o));
-            wzmin = fmin(wzmin, __shfl_xor_sync(0xffffffffu, wzmin, o));
-            wzmax = fmax(wzmax, __shfl_xor_sync(0xffffffffu, wzmax, o));
+        for (int q = 16; q > 0; q >>= 1) {
+            wxmin = fmin(wxmin, __shfl_xor_sync(0xffffffffu, wxmin, q));
+            wxmax = fmax(wxmax, __shfl_xor_sync(0xffffffffu, wxmax, q));
+            wzmin = fmin(wzmin, __shfl_xor_sync(0xffffffffu, wzmin, q));
+            wzmax = fmax(wzmax, __shfl_xor_sync(0xffffffffu, wzmax, q));
         }
-        float su[kBsR], cu[kBsR], sw[kBsR], cw[kBsR];
+        // the warp's target box lives in shared memory (registers go to the pair loop)
+        if (lane == 0) {
+            s_box[wid][0] = wxmin;
+            s_box[wid][1] = wxmax;
+            s_box[wid][2] = wzmin;
+            s_box[wid][3] = wzmax;
+        }
+        float su[kWR], cu[kWR], sw[kWR], cw[kWR];  // Kahan sums of -u and w
 #pragma unroll
-        for (int r = 0; r < kBsR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
+        for (int r = 0; r < kWR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
 
         for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
-            __syncthreads();
-            const uint32_t j = s0 + tid;
-            if (j < j1) {
-                const double4 p = P[j];
-                const double s2 = p.w * p.w;
-                s_src[tid] = make_float4((float)(p.x - ox), (float)(p.y - oz), (float)p.z,
-                                         (float)(10.0 * s2));
-                s_rs[tid] = (float)(1.0 / s2);
-            } else {
-                s_src[tid] = make_float4(1e18f, 1e18f, 0.0f, -1.0f);
-                s_rs[tid] = 0.0f;
+            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < kBsST / 32; ++q) {
+                const uint32_t jj = q * 32 + lane, j = s0 + jj;
+                StagedSrc v;
+                if (j < j1) {
+                    const double2 p = X[j];
+                    const float4 f = F[j];  // (circ, 10 sigma^2, 1/sigma^2, -)
+                    const float px = (float)(p.x - o.x), pz = (float)(p.y - o.y);
+                    v.a = make_float4(px, px, pz, pz);
+                    v.b = make_float4(f.x, f.x, f.y, f.z);
+                } else {  // padding: far away, no circulation, never in a core
+                    v.a = make_float4(1e18f, 1e18f, 1e18f, 1e18f);
+                    v.b = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+                }
+                wsrc[jj] = v;
             }
-            __syncthreads();
+            __syncwarp();
             const TileMeta m = meta[(e.coff + s0) / kBsST];
-            const double gx = fmax(0.0, fmax(m.xmin - wxmax, wxmin - m.xmax));
-            const double gz = fmax(0.0, fmax(m.zmin - wzmax, wzmin - m.zmax));
-            float pu[kBsR], pw[kBsR];
+            const double gx = fmax(0.0, fmax(m.xmin - s_box[wid][1], s_box[wid][0] - m.xmax));
+            const double gz = fmax(0.0, fmax(m.zmin - s_box[wid][3], s_box[wid][2] - m.zmax));
+            uint64_t nu2[kWP], w2[kWP];
 #pragma unroll
-            for (int r = 0; r < kBsR; ++r) pu[r] = pw[r] = 0.0f;
+            for (int q = 0; q < kWP; ++q) nu2[q] = w2[q] = 0ull;  // +0.0f in both halves
             if (gx * gx + gz * gz > m.thr * 1.001 + 1e-30) {
-                stage_far(s_src, tx, tz, pu, pw);
+                stage_far(wsrc, tx2, tz2, nu2, w2);
             } else {
-                stage_near(s_src, s_rs, tx, tz, pu, pw, (int)tb, (int)s0);
+                stage_near(wsrc, tx2, tz2, nu2, w2);
             }
 #pragma unroll
-            for (int r = 0; r < kBsR; ++r) {  // Kahan fold of the stage partial
-                float y = pu[r] - cu[r];
-                float t = su[r] + y;
-                cu[r] = (t - su[r]) - y;
-                su[r] = t;
-                y = pw[r] - cw[r];
-                t = sw[r] + y;
-                cw[r] = (t - sw[r]) - y;
-                sw[r] = t;
+            for (int q = 0; q < kWP; ++q) {  // Kahan fold of the stage partials
+                kahan(su[2 * q], cu[2 * q], f2lo(nu2[q]));
+                kahan(su[2 * q + 1], cu[2 * q + 1], f2hi(nu2[q]));
+                kahan(sw[2 * q], cw[2 * q], f2lo(w2[q]));
+                kahan(sw[2 * q + 1], cw[2 * q + 1], f2hi(w2[q]));
             }
         }
         double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
 #pragma unroll
-        for (int r = 0; r < kBsR; ++r)
+        for (int r = 0; r < kWR; ++r)
             if (tb + r < n)
-                out[tb + r] = make_double2((double)su[r] - (double)cu[r],
+                out[tb + r] = make_double2(-((double)su[r] - (double)cu[r]),
                                            (double)sw[r] - (double)cw[r]);
     }
 }
@@ -326,7 +466,7 @@ __global__ void __launch_bounds__(kBsThreads, 1)
     __shared__ double4 s_src[kBsST];  // x, z, circ, threshold
     __shared__ double s_rs[kBsST];
     __shared__ unsigned s_item;
-    item_prefix_self(s_pre, st, list, nlist);
+    item_prefix_f64(s_pre, st, list, nlist);
     const unsigned total = s_pre[nlist];
     const int tid = threadIdx.x;
     for (;;) {
@@ -493,7 +633,7 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                     const float r2 = fmaf(dx, dx, dz * dz);
                     if (J.skip_close && !(r2 > 1e-15f)) continue;
                     float K = rcp_approx(r2);
-                    if (r2 < (float)s_thr[jj]) K = -expm1f(-r2 * (float)s_rs[jj]) * K;
+                    if (r2 < (float)s_thr[jj]) K = core_kernel(r2, (float)s_rs[jj], K);
                     const float g = K * (float)s_c[jj];
                     pu = fmaf(-g, dz, pu);
                     pw = fmaf(g, dx, pw);
@@ -627,7 +767,10 @@ void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* 
                                         ws.perm, (int64_t)ws.total_cap, 0, ws.key_bits, s);
         perm = ws.perm;
     }
-    k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, ws.meta);
+    double2* pxz = precision == kF32 ? reinterpret_cast<double2*>(ws.packed) : nullptr;
+    float4* pf = precision == kF32 ? reinterpret_cast<float4*>(ws.packed + ws.packed_cap / 2)
+                                   : nullptr;
+    k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, pxz, pf, ws.meta);
     cudaMemsetAsync(ws.work, 0, sizeof(unsigned), s);
 }
 
@@ -635,8 +778,10 @@ void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* 
                          int precision, const Workspace& ws, int sms, cudaStream_t s) {
     (void)table;
     if (precision == kF32)
-        k_self_f32<<<sms * 2, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.meta, ws.part,
-                                                  ws.work);
+        k_self_f32<<<sms * DVM_SELF_MINBLOCKS, 32 * kWWarps, 0, s>>>(
+            st, list, nlist, reinterpret_cast<const double2*>(ws.packed),
+            reinterpret_cast<const float4*>(ws.packed + ws.packed_cap / 2), ws.meta, ws.part,
+            ws.work);
     else
         k_self_f64<<<sms, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part, ws.work);
 }

@@ -13,7 +13,7 @@ from dataclasses import dataclass
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libdvm_cuda.so")
+LIB_PATH = os.environ.get("DVMPP_CUDA_LIB") or os.path.join(HERE, "lib", "libdvm_cuda.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "dvm_cuda.h")
 
 OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_CAPACITY, ERR_RELEASE, ERR_STATE, ERR_RNG, ERR_NO_DEVICE = range(10)

@@ -103,6 +103,21 @@ def test_self_f32_clustered_boundary_layer(ctx, port):
     assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
 
 
+def test_f32_blobs_closer_than_fp32_resolution(ctx, port):
+    """Nascent blobs of one panel can land closer than FP32 resolves; the FP64
+    reference is finite there (K -> 1/sigma^2), so the FP32 path must be too."""
+    x, z, g, s = W.wake(3000, 9, 0.0818804)
+    x = np.concatenate([x, x[:50] + 1e-10, x[50:60] + 3e-8])
+    z = np.concatenate([z, z[:50], z[50:60] - 2e-8])
+    g = np.concatenate([g, g[:60]])
+    s = np.full(x.size, 0.0818804)
+    u0, w0 = port.direct_self(x, z, g, s)
+    assert np.all(np.isfinite(u0))
+    u, w = ctx.biot_savart_self(x, z, g, s, N.F32)
+    assert np.all(np.isfinite(u)) and np.all(np.isfinite(w))
+    assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
+
+
 def test_coincident_distinct_blobs_match_reference_nan(ctx, port):
     """Two distinct blobs at the same point: the reference divides 0/0 (NaN)."""
     x, z = [0.0, 0.0, 1.0], [0.0, 0.0, 0.0]
