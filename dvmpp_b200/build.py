@@ -23,7 +23,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 CUDA_SO = os.path.join(LIB_DIR, "libdvm_cuda.so")
 HOST_SO = os.path.join(LIB_DIR, "libdvmpp_host.so")
 
-CU_SOURCES = ["k_biot_savart.cu", "k_sheet.cu", "k_book.cu", "dvm_capi.cu"]
+CU_SOURCES = ["k_biot_savart.cu", "k_sheet.cu", "k_book.cu", "dvm_capi.cu", "dvm_serve.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
@@ -62,7 +62,7 @@ def build_cuda(verbose=False, force=False) -> str:
     objs = []
     for src in CU_SOURCES:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
         if force or _stale(o, [s] + headers):
             _run([nvcc, *ARCH, *NVCC_FLAGS, "-c", s, "-o", o], verbose)
         objs.append(o)

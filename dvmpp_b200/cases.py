@@ -71,6 +71,42 @@ def run_nbody(n: int, precs, reps: int, seed: int = 2):
     return out
 
 
+def serve_params(r) -> N.Params:
+    """Parameters of one serving request (Philox walk, FP32 pair sums, REFLECT);
+    capacity: the blobs its steps can release, with a 2x margin."""
+    M = 3
+    return N.Params(nu=r["nu"], ux=r["ux"], dt=0.005, max_numpanelvort=M, rng=N.RNG_PHILOX,
+                    precision=N.F32, seed=r["seed"], surface_cross=N.REFLECT,
+                    capacity=r["steps"] * (M + 1) * r["npanels"] * 2 + 1024)
+
+
+def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, max_active: int,
+                budget_gb: float, realtime: bool, serial_too: bool, graph: bool = True,
+                sync: bool = True):
+    """The serving workload, continuous batching and (optionally) the plain
+    serial path on the same requests; returns both summaries."""
+    reqs = W.serving_requests(count, seed, rate, steps_range, panels_range)
+    out = {"workload": "serving", "requests": count, "rate_per_s": rate,
+           "steps_range": list(steps_range), "panels_range": list(panels_range),
+           "budget_gb": budget_gb, "realtime": realtime}
+    modes = [("batched", False)] + ([("serial", True)] if serial_too else [])
+    for name, serial in modes:
+        ctx = N.Context(0)
+        srv = N.Server(ctx, budget_bytes=int(budget_gb * 2**30), max_active=max_active)
+        srv.set_option(N.SERVE_GRAPH, 1 if graph else 0)
+        srv.set_option(N.SERVE_SYNC, 1 if sync else 0)
+        for r in reqs:
+            srv.submit(serve_params(r), *r["body"], r["steps"], r["arrival"])
+        srv.run(serial=serial, realtime=realtime)
+        out[name] = srv.stats()
+        srv.close()
+        ctx.close()
+    if serial_too:
+        out["speedup_sim_steps"] = (out["batched"]["sim_steps_per_s"]
+                                    / max(out["serial"]["sim_steps_per_s"], 1e-12))
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -79,7 +115,23 @@ def main(argv=None):
     nb.add_argument("--prec", choices=["f32", "f64", "both"], default="f32")
     nb.add_argument("--reps", type=int, default=3)
     nb.add_argument("--seed", type=int, default=2)
+    sv = sub.add_parser("serve")
+    sv.add_argument("--requests", type=int, default=100)
+    sv.add_argument("--seed", type=int, default=7)
+    sv.add_argument("--rate", type=float, default=20.0)
+    sv.add_argument("--steps", type=int, nargs=2, default=[100, 2000])
+    sv.add_argument("--panels", type=int, nargs=2, default=[64, 512])
+    sv.add_argument("--max-active", type=int, default=256)
+    sv.add_argument("--budget-gb", type=float, default=150.0)
+    sv.add_argument("--realtime", action="store_true")
+    sv.add_argument("--serial", action="store_true", help="also run the plain serial path")
+    sv.add_argument("--no-graph", action="store_true")
+    sv.add_argument("--no-sync", action="store_true")
     a = ap.parse_args(argv)
+    if a.cmd == "serve":
+        print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
+                                     a.max_active, a.budget_gb, a.realtime, a.serial,
+                                     not a.no_graph, not a.no_sync)))
     if a.cmd == "nbody":
         precs = {"f32": [N.F32], "f64": [N.F64], "both": [N.F32, N.F64]}[a.prec]
         print(json.dumps(run_nbody(a.n, precs, a.reps, a.seed)))

@@ -46,6 +46,8 @@ namespace {
     } while (0)
 
 constexpr int kTableCap = 4096;
+constexpr size_t kMaxPlans = 32;       // cached batch plans per context (LRU)
+constexpr size_t kPoolPerPlan = 4096;  // list entries per plan: 4 partitions x 1024 sims
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -55,7 +57,7 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // (>= ~2^21 / cap items per 256-target tile) to occupy the GPU when stepped
 // alone, but never chunks shorter than 8 k sources.
 int nbody_chunks(uint32_t cap) {
-    const int by_size = (int)((cap + 65535) / 65536);
+    const int by_size = (int)std::min<uint32_t>(16, (cap + 65535) / 65536);
     const int by_fill = (int)((2u << 20) / std::max<uint32_t>(cap, 1));
     const int most = (int)std::max<uint32_t>(1, std::min<uint32_t>(64, cap / 8192));
     return std::max(1, std::min(most, std::max(by_size, by_fill)));
@@ -82,6 +84,9 @@ struct Plan {
     uint64_t ws_generation = 0;
     uint64_t launches_per_step = 0;
     bool warmed = false;  // one eager step issued (kernel attributes set, buffers touched)
+    uint64_t last_use = 0;
+    int pool_slot = -1;   // slot of the context's list pool holding the sublists
+    int pool_used = 0;
 };
 
 struct dvm_ctx {
@@ -105,6 +110,9 @@ struct dvm_ctx {
     void* raw_block = nullptr;
     size_t raw_bytes = 0;
     std::map<std::vector<int>, Plan*> plans;
+    uint64_t plan_clock = 0;
+    ListEntry* list_pool = nullptr;  // kMaxPlans slots of kPoolPerPlan entries
+    std::vector<int> pool_free;
     std::mutex mu;
     // CUDA-event profiling of kernel families on the ctx stream (eager steps only)
     bool profiling = false;
@@ -136,21 +144,18 @@ struct dvm_sim {
 namespace {
 
 // ---- plans ------------------------------------------------------------------------
-void free_plan(Plan* pl) {
+void free_plan(dvm_ctx* c, Plan* pl) {
     if (!pl) return;
     if (pl->exec) cudaGraphExecDestroy(pl->exec);
     if (pl->graph) cudaGraphDestroy(pl->graph);
-    SubList* subs[] = {&pl->all, &pl->euler, &pl->rk3, &pl->rk3_f32, &pl->rk3_f64,
-                       &pl->eul_f32, &pl->eul_f64, &pl->refl, &pl->del};
-    for (SubList* s : subs)
-        if (s->d_list) cudaFree(s->d_list);
+    if (pl->pool_slot >= 0) c->pool_free.push_back(pl->pool_slot);  // list memory is pooled
     delete pl;
 }
 
 void drop_plans_with(dvm_ctx* c, int slot) {
     for (auto it = c->plans.begin(); it != c->plans.end();) {
         if (slot < 0 || std::find(it->first.begin(), it->first.end(), slot) != it->first.end()) {
-            free_plan(it->second);
+            free_plan(c, it->second);
             it = c->plans.erase(it);
         } else {
             ++it;
@@ -187,8 +192,12 @@ int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl) {
     pl.part_elems = std::max(pl.part_elems, poff);
     pl.rhs_elems = std::max(pl.rhs_elems, roff);
     pl.circ_elems = std::max(pl.circ_elems, cofs);
-    CK(cudaMalloc(&sl.d_list, sizeof(ListEntry) * sl.n));
-    CK(cudaMemcpy(sl.d_list, h.data(), sizeof(ListEntry) * sl.n, cudaMemcpyHostToDevice));
+    // The plan's lists live in its slot of the context's list pool; the copy is
+    // ordered on the stream after every kernel that read the slot before.
+    sl.d_list = c->list_pool + (size_t)pl.pool_slot * kPoolPerPlan + pl.pool_used;
+    pl.pool_used += sl.n;
+    CK(cudaMemcpyAsync(sl.d_list, h.data(), sizeof(ListEntry) * sl.n, cudaMemcpyHostToDevice,
+                       c->stream));
     return DVM_OK;
 }
 
@@ -396,10 +405,22 @@ void issue_step(dvm_ctx* c, Plan& pl) {
 int get_plan(dvm_ctx* c, const std::vector<int>& slots, Plan** out) {
     auto it = c->plans.find(slots);
     if (it != c->plans.end()) {
+        it->second->last_use = ++c->plan_clock;
         *out = it->second;
         return DVM_OK;
     }
+    if (c->plans.size() >= kMaxPlans) {  // a serving loop changes its batch often
+        auto victim = c->plans.begin();
+        for (auto jt = c->plans.begin(); jt != c->plans.end(); ++jt)
+            if (jt->second->last_use < victim->second->last_use) victim = jt;
+        free_plan(c, victim->second);
+        c->plans.erase(victim);
+    }
+    if (c->pool_free.empty()) return fail(DVM_ERR_STATE, "no free plan slot");
     Plan* pl = new Plan();
+    pl->pool_slot = c->pool_free.back();
+    c->pool_free.pop_back();
+    pl->last_use = ++c->plan_clock;
     pl->slots = slots;
     for (int sl : slots) {
         const dvm_sim* s = c->slots[sl];
@@ -420,7 +441,7 @@ int get_plan(dvm_ctx* c, const std::vector<int>& slots, Plan** out) {
     for (SubList* s : subs) {
         const int rc = build_sublist(c, *s, *pl);
         if (rc) {
-            free_plan(pl);
+            free_plan(c, pl);
             return rc;
         }
     }
@@ -556,6 +577,8 @@ int dvm_ctx_create(int device, uint64_t budget, dvm_ctx** out) {
     if (e == cudaSuccess) e = cudaMalloc(&c->d_table, sizeof(InstDesc) * kTableCap);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_state, sizeof(InstState) * kTableCap);
     if (e == cudaSuccess) e = cudaMemset(c->d_state, 0, sizeof(InstState) * kTableCap);
+    if (e == cudaSuccess) e = cudaMalloc(&c->list_pool, sizeof(ListEntry) * kMaxPlans * kPoolPerPlan);
+    for (int i = (int)kMaxPlans - 1; i >= 0; --i) c->pool_free.push_back(i);
     if (e != cudaSuccess) {
         dvm_ctx_destroy(c);
         return fail(DVM_ERR_CUDA, std::string("ctx create: ") + cudaGetErrorString(e));
@@ -585,6 +608,7 @@ int dvm_ctx_destroy(dvm_ctx* c) {
         if (e) cudaEventDestroy(e);
     if (c->ws_block) cudaFree(c->ws_block);
     if (c->raw_block) cudaFree(c->raw_block);
+    if (c->list_pool) cudaFree(c->list_pool);
     if (c->d_table) cudaFree(c->d_table);
     if (c->d_state) cudaFree(c->d_state);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -610,6 +634,26 @@ int dvm_ctx_device_info(dvm_ctx* c, int* sms, int* ma, int* mi) {
     if (sms) *sms = c->sms;
     if (ma) *ma = c->cc_major;
     if (mi) *mi = c->cc_minor;
+    return DVM_OK;
+}
+
+int dvm_ctx_reserve(dvm_ctx* c, uint64_t total_capacity, int max_sims, int max_panels,
+                    int with_delete) {
+    if (!c || max_sims < 1 || max_panels < 2) return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    const uint64_t S = (uint64_t)max_sims;
+    const uint64_t T = align_up(total_capacity, kCapAlign) + S * kCapAlign;
+    // bounds of the per-list sums: chunks*cap <= 16 cap + 2^21, rhs chunks <= cap/4096 + 1
+    const uint64_t part = 16 * T + S * (2u << 20);
+    const uint64_t rchunks = T / kAtChunk + S;
+    return ensure_workspace(c, T, part, rchunks * align_up((size_t)max_panels, 256), rchunks,
+                            max_sims, with_delete != 0);
+}
+
+int dvm_ctx_workspace_bytes(dvm_ctx* c, uint64_t* bytes) {
+    if (!c || !bytes) return fail(DVM_ERR_ARG, "null argument");
+    *bytes = c->ws_bytes;
     return DVM_OK;
 }
 

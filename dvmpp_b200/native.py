@@ -371,3 +371,91 @@ class Simulation:
 
     def step(self, nsteps: int = 1):
         _check(self.lib.dvm_sim_step(self.h, nsteps))
+
+
+# ---- serving ----------------------------------------------------------------
+SERVE_GRAPH, SERVE_SYNC = 0, 1
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("arrival_s", C.c_double), ("admitted_s", C.c_double),
+                ("finished_s", C.c_double), ("latency_s", C.c_double), ("steps_done", C.c_uint32),
+                ("status", C.c_int32), ("blobs", C.c_uint64), ("fx", C.c_double),
+                ("fz", C.c_double), ("cd", C.c_double), ("cl", C.c_double)]
+
+
+class ServerSummary(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("sim_steps", C.c_uint64), ("ticks", C.c_uint64), ("wall_s", C.c_double),
+                ("sim_steps_per_s", C.c_double), ("latency_p50_s", C.c_double),
+                ("latency_p95_s", C.c_double), ("latency_p99_s", C.c_double),
+                ("latency_mean_s", C.c_double), ("queue_p50_s", C.c_double),
+                ("queue_p99_s", C.c_double), ("peak_active", C.c_uint32),
+                ("peak_bytes", C.c_uint64)]
+
+
+SIGNATURES.update({
+    "dvm_ctx_reserve": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int]),
+    "dvm_ctx_workspace_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "dvm_server_create": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "dvm_server_destroy": (C.c_int, [C.c_void_p]),
+    "dvm_server_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dvm_server_submit": (C.c_int, [C.c_void_p, C.POINTER(SimParams), _dp, _dp, C.c_int, C.c_uint32,
+                                    C.c_double, C.POINTER(C.c_uint64)]),
+    "dvm_server_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dvm_server_result": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(RequestResult)]),
+    "dvm_server_final_blobs": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
+                                         _dp, _dp, _dp]),
+    "dvm_server_stats": (C.c_int, [C.c_void_p, C.POINTER(ServerSummary)]),
+})
+
+
+class Server:
+    """Continuous-batching request loop over one Context (dvm_server)."""
+
+    def __init__(self, ctx: Context, budget_bytes: int = 0, max_active: int = 64, keep_state=False):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        _check(self.lib.dvm_server_create(ctx.h, budget_bytes, max_active, 1 if keep_state else 0,
+                                          C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and getattr(self.ctx, "h", None):
+            self.lib.dvm_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def set_option(self, option: int, value: int):
+        _check(self.lib.dvm_server_set_option(self.h, option, value))
+
+    def submit(self, params: Params, xp, zp, steps: int, arrival_s: float = 0.0) -> int:
+        xp, zp = _f64(xp), _f64(zp)
+        cp = params.c()
+        rid = C.c_uint64()
+        _check(self.lib.dvm_server_submit(self.h, C.byref(cp), _p(xp), _p(zp), xp.size, steps,
+                                          arrival_s, C.byref(rid)))
+        return rid.value
+
+    def run(self, serial=False, realtime=False):
+        _check(self.lib.dvm_server_run(self.h, 1 if serial else 0, 1 if realtime else 0))
+
+    def result(self, rid: int) -> dict:
+        r = RequestResult()
+        _check(self.lib.dvm_server_result(self.h, rid, C.byref(r)))
+        return {f: getattr(r, f) for f, _ in RequestResult._fields_}
+
+    def final_blobs(self, rid: int):
+        n = C.c_uint64()
+        _check(self.lib.dvm_server_final_blobs(self.h, rid, 0, C.byref(n), None, None, None))
+        x, z, c = np.empty(n.value), np.empty(n.value), np.empty(n.value)
+        _check(self.lib.dvm_server_final_blobs(self.h, rid, n.value, C.byref(n), _p(x), _p(z), _p(c)))
+        return x, z, c
+
+    def stats(self) -> dict:
+        s = ServerSummary()
+        _check(self.lib.dvm_server_stats(self.h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in ServerSummary._fields_}

@@ -149,3 +149,33 @@ def batched_instances(count: int = 64, seed: int = 4):
         x, z, g, s = wake(nb, seed * 1000 + k, sig, scale=R / 0.5)
         out.append(dict(kind=kind, npanels=npan, nblobs=nb, body=(bx, bz), blobs=(x, z, g, s)))
     return out
+
+
+def serving_requests(count: int = 1000, seed: int = 7, rate_per_s: float = 20.0,
+                     steps_range=(100, 2000), panels_range=(64, 512)):
+    """Requests of the serving workload: Poisson arrivals at `rate_per_s`;
+    bodies from {circle R=0.5, ellipse aspect U[1,4], rounded square,
+    Joukowski thickness U[0.08,0.16] at AoA U[0,15] deg}; panels U{64..512};
+    nu log-uniform [1e-4, 1e-2]; ux U[1,3]; steps U{100..2000}; dt 0.005;
+    REFLECT; each simulation starts with no blobs."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(count):
+        t += rng.exponential(1.0 / rate_per_s)
+        kind = ("circle", "ellipse", "rsquare", "joukowski")[int(rng.integers(0, 4))]
+        npan = int(rng.integers(panels_range[0], panels_range[1] + 1))
+        if kind == "circle":
+            bx, bz = circle(npan)
+        elif kind == "ellipse":
+            bx, bz = ellipse(npan, 0.5, 0.5 / float(rng.uniform(1.0, 4.0)))
+        elif kind == "rsquare":
+            bx, bz = rounded_square(npan)
+        else:
+            bx, bz = joukowski(npan, float(rng.uniform(0.08, 0.16)), float(rng.uniform(0.0, 15.0)))
+        nu = float(math.exp(rng.uniform(math.log(1e-4), math.log(1e-2))))
+        ux = float(rng.uniform(1.0, 3.0))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        out.append(dict(kind=kind, npanels=npan, body=(bx, bz), nu=nu, ux=ux, steps=steps,
+                        arrival=t, seed=int(rng.integers(0, 2**31 - 1))))
+    return out

@@ -138,6 +138,12 @@ int dvm_ctx_launch_count(dvm_ctx* ctx, uint64_t* launches);
 #define DVM_PROF_SORT 7       /* Morton sort, pack, partial combine */
 #define DVM_PROF_STEP 8       /* whole step */
 #define DVM_PROF_FAMILIES 9
+/* Pre-size the shared workspace for batches of up to max_sims simulations whose
+ * capacities sum to total_capacity blobs (avoids allocations, and re-captured
+ * graphs, while a serving loop admits and retires simulations). */
+int dvm_ctx_reserve(dvm_ctx* ctx, uint64_t total_capacity, int max_sims, int max_panels,
+                    int with_delete);
+int dvm_ctx_workspace_bytes(dvm_ctx* ctx, uint64_t* bytes);
 /* Timing markers: dvm_ctx_mark records CUDA event `slot` (0..15) on the ctx
  * stream; dvm_ctx_elapsed synchronises and returns the device time between
  * two recorded markers. */
@@ -224,6 +230,57 @@ int dvm_sim_step(dvm_sim* sim, int nsteps);
  * of them in one launch.  use_graph != 0 captures the step in a CUDA graph
  * (re-used while the list is unchanged).  Asynchronous: check dvm_sim_status. */
 int dvm_step_batch(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int nsteps, int use_graph);
+
+/* ---- serving (no counterpart in the reference) ----------------------------------------
+ * A request loop over one context: requests (a body, parameters and a step
+ * count) arrive at given times; each is admitted as soon as it has arrived,
+ * a batch slot is free and its slab fits the HBM budget (FIFO, no overtaking);
+ * every tick advances ALL admitted simulations by one step in one batched
+ * launch sequence (continuous batching: new requests join while others run);
+ * finished ones are retired immediately and free their memory.  `serial`
+ * runs the same requests one at a time (the plain GPU path) for comparison.
+ * `realtime` != 0 honours arrival times on the wall clock; 0 treats every
+ * request as arrived at t = 0. */
+typedef struct dvm_server dvm_server;
+typedef struct {
+    uint64_t id;
+    double arrival_s, admitted_s, finished_s; /* seconds since the run started */
+    double latency_s;                         /* finished - arrival */
+    uint32_t steps_done;
+    int32_t status;                           /* DVM_OK or the simulation's error */
+    uint64_t blobs;                           /* blob count at the end */
+    double fx, fz, cd, cl;                    /* last loads */
+} dvm_request_result;
+typedef struct {
+    uint64_t requests, completed, failed, sim_steps, ticks;
+    double wall_s, sim_steps_per_s;
+    double latency_p50_s, latency_p95_s, latency_p99_s, latency_mean_s;
+    double queue_p50_s, queue_p99_s;
+    uint32_t peak_active;
+    uint64_t peak_bytes;
+} dvm_server_summary;
+
+/* hbm_budget_bytes: device memory the server's simulations may hold (0: the
+ * context budget minus its workspace).  max_active: batch size limit.
+ * keep_state != 0 keeps every request's final x, z, circ on the host. */
+int dvm_server_create(dvm_ctx* ctx, uint64_t hbm_budget_bytes, int max_active, int keep_state,
+                      dvm_server** out);
+int dvm_server_destroy(dvm_server* srv);
+/* Options (before dvm_server_run): DVM_SERVE_GRAPH 1 captures the step in a CUDA
+ * graph, re-used while the batch is unchanged (default 1); DVM_SERVE_SYNC 1
+ * waits for each tick before the next admission (default 1; 0 lets the host
+ * run ahead and reads device status only at retirement). */
+#define DVM_SERVE_GRAPH 0
+#define DVM_SERVE_SYNC 1
+int dvm_server_set_option(dvm_server* srv, int option, int value);
+int dvm_server_submit(dvm_server* srv, const dvm_sim_params* p, const double* body_x,
+                      const double* body_z, int npoints, uint32_t steps, double arrival_s,
+                      uint64_t* id);
+int dvm_server_run(dvm_server* srv, int serial, int realtime);
+int dvm_server_result(dvm_server* srv, uint64_t id, dvm_request_result* out);
+int dvm_server_final_blobs(dvm_server* srv, uint64_t id, uint64_t cap, uint64_t* n, double* x,
+                           double* z, double* circ);
+int dvm_server_stats(dvm_server* srv, dvm_server_summary* out);
 
 #ifdef __cplusplus
 }

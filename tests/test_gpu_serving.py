@@ -1,0 +1,56 @@
+"""Serving loop (dvm_server_*): continuous batching with HBM-budget admission.
+
+The key property: every request's result is the same alone and in the mix.
+Each simulation's random walk is keyed by its own seed (Philox counters carry
+no batch position) and its pair sums are associated by its own capacity, so
+the final blob state must be bit-identical between a batched run and the
+serial (one request at a time) run of the same requests."""
+import numpy as np
+import pytest
+
+from dvmpp_b200 import native as N
+from dvmpp_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(r, steps):
+    M = 3
+    return N.Params(nu=r["nu"], ux=r["ux"], dt=0.005, max_numpanelvort=M, rng=N.RNG_PHILOX,
+                    precision=N.F32, seed=r["seed"], surface_cross=N.REFLECT,
+                    capacity=steps * (M + 1) * r["npanels"] * 2 + 1024)
+
+
+def _run(ctx, reqs, serial, budget=0, max_active=64):
+    srv = N.Server(ctx, budget_bytes=budget, max_active=max_active, keep_state=True)
+    ids = [srv.submit(_params(r, r["steps"]), *r["body"], r["steps"], r["arrival"]) for r in reqs]
+    srv.run(serial=serial, realtime=False)
+    out = {i: (srv.result(i), srv.final_blobs(i)) for i in ids}
+    st = srv.stats()
+    srv.close()
+    return out, st
+
+
+def test_alone_equals_in_mix(ctx):
+    reqs = W.serving_requests(12, seed=11, steps_range=(5, 30), panels_range=(64, 200))
+    mixed, st_m = _run(ctx, reqs, serial=False)
+    alone, st_a = _run(ctx, reqs, serial=True)
+    assert st_m["completed"] == len(reqs) and st_a["completed"] == len(reqs)
+    assert st_m["peak_active"] > 1 and st_a["peak_active"] == 1
+    for i in mixed:
+        (ra, (xa, za, ca)), (rb, (xb, zb, cb)) = mixed[i], alone[i]
+        assert ra["status"] == 0 and rb["status"] == 0
+        assert ra["steps_done"] == reqs[i]["steps"]
+        assert ra["blobs"] == rb["blobs"] and xa.size == ra["blobs"]
+        assert np.array_equal(xa, xb) and np.array_equal(za, zb) and np.array_equal(ca, cb)
+        assert ra["cd"] == rb["cd"] and ra["cl"] == rb["cl"]
+
+
+def test_admission_respects_hbm_budget(ctx):
+    reqs = W.serving_requests(10, seed=12, steps_range=(5, 15), panels_range=(64, 128))
+    sizes = [N.sim_bytes(_params(r, r["steps"]), r["npanels"]) for r in reqs]
+    budget = int(2.5 * max(sizes))  # at most two or three resident at once
+    _, st = _run(ctx, reqs, serial=False, budget=budget)
+    assert st["completed"] == len(reqs)
+    assert st["peak_bytes"] <= budget
+    assert 1 <= st["peak_active"] <= 3
