@@ -1023,6 +1023,43 @@ int dvm_sim_get_step(dvm_sim* s, uint32_t* step) {
     return DVM_OK;
 }
 
+int dvm_sim_clear_uniforms(dvm_sim* s) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    uint64_t cursor = 0;
+    CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    s->consumed_base += cursor;  // what was consumed stays counted
+    const uint64_t zero = 0;
+    CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].cursor, &zero, 8, cudaMemcpyHostToDevice, s->ctx->stream));
+    s->h.ucount = 0;
+    int rc = upload_desc(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_pending_uniforms(dvm_sim* s, double* out, uint64_t cap, uint64_t* n) {
+    if (!s || !n) return fail(DVM_ERR_ARG, "null argument");
+    uint64_t cursor = 0;
+    CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    const uint64_t avail = s->h.ucount > cursor ? s->h.ucount - cursor : 0;
+    *n = avail;
+    if (!out) return DVM_OK;
+    if (cap < avail) return fail(DVM_ERR_ARG, "output capacity smaller than the pending count");
+    if (avail)
+        CK(cudaMemcpyAsync(out, s->uniforms + cursor, 8 * avail, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
+int dvm_sim_set_step(dvm_sim* s, uint32_t step) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].step, &step, 4, cudaMemcpyHostToDevice, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    return DVM_OK;
+}
+
 int dvm_sim_push_uniforms(dvm_sim* s, const double* u, uint64_t n) {
     if (!s || (n && !u)) return fail(DVM_ERR_ARG, "null argument");
     if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
@@ -1275,6 +1312,28 @@ int dvm_biot_savart_self(dvm_ctx* c, const dvm_particle* p, uint64_t n, dvm_velo
         out[i].u = h[4 * n + i];
         out[i].w = h[5 * n + i];
     }
+    return DVM_OK;
+}
+
+int dvm_random_walk(dvm_ctx* c, double* x, double* z, uint64_t n, const double* R, double nu,
+                    double dt) {
+    if (!c || (n && (!x || !z || !R))) return fail(DVM_ERR_ARG, "null argument");
+    if (n == 0) return DVM_OK;
+    if (n > 0xF0000000ull) return fail(DVM_ERR_ARG, "too many blobs");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    int rc = raw_reserve(c, 8 * 4 * n);
+    if (rc) return rc;
+    double* d = static_cast<double*>(c->raw_block);
+    CK(cudaMemcpyAsync(d, x, 8 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d + n, z, 8 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d + 2 * n, R, 16 * n, cudaMemcpyHostToDevice, c->stream));
+    diffuse_raw(d, d + n, (uint32_t)n, d + 2 * n, nu, dt, c->sms, c->stream);
+    g_launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(x, d, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(z, d + n, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return DVM_OK;
 }
 

@@ -190,6 +190,9 @@ void convect_update(const InstDesc* table, InstState* st, const ListEntry* list,
                     int mode, const Workspace& ws, int sms, cudaStream_t s);
 void diffuse(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
              const Workspace& ws, int sms, cudaStream_t s);
+// src/VortexBlobs.cpp:251-265 on caller device buffers, uniforms R[2i], R[2i+1].
+void diffuse_raw(double* x, double* z, uint32_t n, const double* R, double nu, double dt,
+                 int sms, cudaStream_t s);
 void release(const InstDesc* table, InstState* st, const ListEntry* list, int nlist, int max_np,
              cudaStream_t s);
 void reflect(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,

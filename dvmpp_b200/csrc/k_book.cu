@@ -49,6 +49,19 @@ __global__ void k_diffuse(const InstDesc* __restrict__ table, InstState* __restr
     }
 }
 
+// The same walk on caller buffers with caller uniforms R[2i], R[2i+1].
+__global__ void k_diffuse_raw(double* __restrict__ x, double* __restrict__ z, uint32_t n,
+                              const double* __restrict__ R, double nu, double dt) {
+    const double c4 = dmul(dmul(4.0, nu), dt);
+    const double twopi = dmul(2.0, kPi);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double rrw = sqrt(dmul(c4, log(ddiv(1.0, R[2ull * i]))));
+        const double th = dmul(twopi, R[2ull * i + 1]);
+        x[i] = dadd(x[i], dmul(rrw, cos(th)));
+        z[i] = dadd(z[i], dmul(rrw, sin(th)));
+    }
+}
+
 // ---- release + append: one block per simulation -------------------------------------
 constexpr int kRelThreads = 256;
 
@@ -421,6 +434,13 @@ void diffuse(const InstDesc* table, InstState* st, const ListEntry* list, int nl
     (void)ws;
     dim3 g(std::max(1, sms * 8 / std::max(1, nlist)), nlist);
     k_diffuse<<<g, 256, 0, s>>>(table, st, list, nlist);
+}
+
+void diffuse_raw(double* x, double* z, uint32_t n, const double* R, double nu, double dt,
+                 int sms, cudaStream_t s) {
+    if (n == 0) return;
+    const unsigned g = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sms * 8);
+    k_diffuse_raw<<<g, 256, 0, s>>>(x, z, n, R, nu, dt);
 }
 
 void release(const InstDesc* table, InstState* st, const ListEntry* list, int nlist, int max_np,

@@ -1,0 +1,151 @@
+#include "DVMBase.hpp"
+
+#include <cmath>
+#include <iostream>
+#include <vector>
+
+#include "Device.hpp"
+
+DVMBase::DVMBase(XmlHandler& xml, const std::string& stamp)
+    : m_vortex(xml, stamp), m_vortsheet(xml, stamp), m_probe(xml, stamp), m_xml(xml) {
+    m_nu = xml.getValueAttribute("constants", "nu");
+    m_dt = xml.getValueAttribute("time", "dt");
+    m_steps = static_cast<unsigned>(xml.getValueAttribute("time", "steps"));
+    m_Ux = xml.getValueAttribute("flow", "ux");
+    m_Uz = xml.getValueAttribute("flow", "uz");
+    m_Ur = std::sqrt(m_Ux * m_Ux + m_Uz * m_Uz);
+    const int seed = xml.getIntAttribute("constants", "seed");
+    m_rand.seed(seed);
+    const std::string scheme = xml.getStringAttribute("time", "scheme");
+    m_scheme = scheme == "RK3" ? Scheme::RK3 : Scheme::Euler;
+    const std::string sc = xml.getStringAttribute("algorithms", "surface_crossing");
+    m_surfcross = sc == "DELETE" ? SurfaceCross::Delete
+                                 : (sc == "ABSORB" ? SurfaceCross::Absorb : SurfaceCross::Reflect);
+    if (xml.has("algorithms", "velocity_kernel")) {
+        const std::string k = xml.getStringAttribute("algorithms", "velocity_kernel");
+        m_precision = (k == "cuda") ? DVM_F32 : DVM_F64;
+        m_vortex.setKernelType(k == "fmm" ? "direct" : k);
+    }
+    if (xml.has("algorithms", "diffusion_rng"))
+        m_rng_mode = xml.getStringAttribute("algorithms", "diffusion_rng") == "philox"
+                         ? DVM_RNG_PHILOX
+                         : DVM_RNG_INJECT;
+    if (xml.has("algorithms", "merge_frequency") && xml.getValueAttribute("algorithms", "merge_frequency") > 0)
+        std::cout << "Vortex merging is not part of this build; merge options are ignored"
+                  << std::endl;
+    if (xml.has("remesh", "frequency"))
+        std::cout << "Remeshing is not part of this build; <remesh> is ignored" << std::endl;
+    const int cross = m_surfcross == SurfaceCross::Delete
+                          ? DVM_DELETE
+                          : (m_surfcross == SurfaceCross::Absorb ? DVM_ABSORB : DVM_REFLECT);
+    m_vortsheet.set_params(m_precision, m_rng_mode,
+                           m_scheme == Scheme::RK3 ? DVM_RK3 : DVM_EULER, cross, seed);
+    m_sim = m_vortsheet.device(0);
+}
+
+unsigned DVMBase::get_steps() const { return m_steps; }
+double DVMBase::get_time() const { return m_time; }
+
+void DVMBase::increment_step() {
+    m_step++;
+    m_time = m_step * m_dt;
+}
+
+void DVMBase::supply_uniforms() {
+    // Inject mode: keep at least this step's draws on the device -- 2N for the
+    // walk plus the release -- as the next values of the reference's stream.
+    if (m_rng_mode != DVM_RNG_INJECT) return;
+    uint64_t n = 0, consumed = 0, avail = 0;
+    dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "DVMBase");
+    dvm::check_status(dvm_sim_rng_position(m_sim, &consumed, &avail), "DVMBase");
+    const uint64_t need = 2 * n + m_vortsheet.max_release();
+    if (avail >= need) return;
+    std::vector<double> u(need - avail + 2 * n + 4096);  // a little ahead
+    for (auto& v : u) v = m_rand.rand();
+    dvm::check_status(dvm_sim_push_uniforms(m_sim, u.data(), u.size()), "DVMBase");
+}
+
+void DVMBase::compute_step() {
+    // Grow the device simulation when the next releases might not fit: copy
+    // the state out, rebuild with twice the room, and restore it (including the
+    // not-yet-consumed part of the random stream).
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "DVMBase");
+    const uint64_t need = n + m_vortsheet.max_release();
+    if (need > m_vortsheet.capacity()) {
+        std::vector<double> pending;
+        if (m_rng_mode == DVM_RNG_INJECT) {
+            uint64_t np = 0;
+            dvm::check_status(dvm_sim_pending_uniforms(m_sim, nullptr, 0, &np), "DVMBase");
+            pending.resize(np);
+            if (np)
+                dvm::check_status(dvm_sim_pending_uniforms(m_sim, pending.data(), np, &np),
+                                  "DVMBase");
+        }
+        sync_to_host();
+        m_sim = m_vortsheet.device(need);
+        dvm::check_status(dvm_sim_set_blobs(m_sim, m_vortex.size(), dvm::vec_ptr(m_vortex.m_x),
+                                            dvm::vec_ptr(m_vortex.m_z),
+                                            dvm::vec_ptr(m_vortex.m_circ),
+                                            dvm::vec_ptr(m_vortex.m_sigma)),
+                          "DVMBase");
+        dvm::check_status(dvm_sim_set_step(m_sim, m_step - 1), "DVMBase");
+        if (!pending.empty())
+            dvm::check_status(dvm_sim_push_uniforms(m_sim, pending.data(), pending.size()),
+                              "DVMBase");
+    }
+    supply_uniforms();
+    // convect (Euler or RK3), remesh (off), diffusion, release + append,
+    // surface crossing, loads: src/DVMBase.cpp:86-133, one batched sequence
+    dvm::check_status(dvm_sim_step(m_sim, 1), "DVMBase::compute_step");
+    dvm::check_status(dvm_sim_status(m_sim), "DVMBase::compute_step");
+}
+
+void DVMBase::convect() { dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_CONVECT), "convect"); }
+
+void DVMBase::remesh() {}
+
+void DVMBase::sync_to_host() {
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "DVMBase");
+    m_vortex.resize((unsigned)n);
+    std::vector<uint32_t> ids(n);
+    dvm::check_status(
+        dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(m_vortex.m_x), dvm::vec_ptr(m_vortex.m_z),
+                          dvm::vec_ptr(m_vortex.m_circ), dvm::vec_ptr(m_vortex.m_sigma),
+                          dvm::vec_ptr(m_vortex.m_u), dvm::vec_ptr(m_vortex.m_w),
+                          dvm::vec_ptr(m_vortex.m_uvs), dvm::vec_ptr(m_vortex.m_wvs), ids.data()),
+        "DVMBase");
+    for (uint64_t i = 0; i < n; ++i) m_vortex.m_ID[i] = ids[i];
+    m_vortsheet.pull_from_device();
+}
+
+void DVMBase::write_outputs() {
+    m_vortex.write_step(m_time, m_step);
+    m_vortsheet.write_step(m_time);
+    m_probe.write_step(m_time);
+}
+
+void DVMBase::run(unsigned steps, bool write, bool quiet) {
+    m_quiet = quiet;
+    for (unsigned j = 1; j <= steps; j++) {
+        increment_step();
+        compute_step();
+        if (write || !quiet || j == steps) sync_to_host();
+        if (write) write_outputs();
+        if (!quiet) {
+            double fx = 0, fz = 0, cd = 0, cl = 0;
+            dvm_sim_get_loads(m_sim, &fx, &fz, &cd, &cl);
+            std::cout << "C_D = " << cd << "\tC_L = " << cl << std::endl;
+            std::cout << "Simulation time          = " << get_time() << "\tStep " << j << "/"
+                      << steps << std::endl;
+            std::cout << "Number of vortex blobs   = " << m_vortex.size() << std::endl;
+        }
+    }
+}
+
+void DVMBase::solve() { run(get_steps(), true, false); }
+
+unsigned DVMBase::num_blobs() const { return m_vortex.size(); }
+
+std::tuple<double, double> DVMBase::forces() const { return m_vortsheet.get_forces(); }

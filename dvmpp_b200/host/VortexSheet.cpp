@@ -1,0 +1,285 @@
+#include "VortexSheet.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <filesystem>
+#include <iostream>
+#include <vector>
+
+#include "Device.hpp"
+
+namespace fs = std::filesystem;
+
+VortexSheet::VortexSheet() = default;
+
+VortexSheet::VortexSheet(const XmlHandler& xml, const std::string& stamp) {
+    m_rho = xml.getValueAttribute("constants", "density");
+    m_nu = xml.getValueAttribute("constants", "nu");
+    m_dt = xml.getValueAttribute("time", "dt");
+    m_Ux = xml.getValueAttribute("flow", "ux");
+    m_Uz = xml.getValueAttribute("flow", "uz");
+    m_maxNumPanelVort = static_cast<unsigned>(xml.getValueAttribute("constants", "max_NumPanelVort"));
+    m_cutoff_exp = xml.getValueAttribute("constants", "cutoff_exp");
+    const fs::path inpath(xml.getStringAttribute("io", "input_dir"));
+    read_input_coord((inpath / xml.getStringAttribute("io", "domain_file")).string());
+
+    m_params.rho = m_rho;
+    m_params.nu = m_nu;
+    m_params.dt = m_dt;
+    m_params.ux = m_Ux;
+    m_params.uz = m_Uz;
+    m_params.cutoff_exp = m_cutoff_exp;
+    m_params.max_numpanelvort = m_maxNumPanelVort;
+    m_params.scheme = DVM_EULER;
+    m_params.surface_cross = DVM_REFLECT;
+    m_params.rng = DVM_RNG_INJECT;
+    m_params.precision = DVM_F64;
+    m_params.seed = 0;
+    const double steps = xml.getValueAttribute("time", "steps");
+    const double npanels = (double)m_x.n_elem - 1.0;
+    build_device((uint64_t)(steps * 2.0 * (m_maxNumPanelVort + 1) * npanels) + 4096);
+
+    const std::string outdir = xml.getStringAttribute("io", "output_dir", true);
+    const auto gamma_path = fs::path(outdir) / (stamp + "_gamma.dat");
+    m_gammafile.open(gamma_path);
+    if (!m_gammafile) throw dvm::FileIOException::cannotOpen(gamma_path.string());
+    // headers of src/VortexSheet.cpp:43-53
+    m_gammafile << m_xc.n_elem << " # Number of collocation points\n"
+                << m_dt << " # Time Step\n"
+                << steps << " # Steps\n"
+                << "Time [s] Gamma - Vortex sheet strength\n";
+    const auto force_path = fs::path(outdir) / (stamp + "_loads.dat");
+    m_forcefile.open(force_path);
+    if (!m_forcefile) throw dvm::FileIOException::cannotOpen(force_path.string());
+    m_forcefile << "Time [s]\tF_x [-]\tF_z [s]\n";
+}
+
+VortexSheet::~VortexSheet() {
+    if (m_sim) dvm_sim_destroy(m_sim);
+}
+
+void VortexSheet::read_input_coord(const std::string& file) {
+    // two numbers per line, blank lines ignored (the reference's raw_ascii load)
+    std::ifstream f(file);
+    if (!f) throw dvm::FileIOException::cannotRead(file);
+    std::vector<double> xs, zs;
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream s(line);
+        std::vector<double> v;
+        double d;
+        while (s >> d) v.push_back(d);
+        if (v.empty()) continue;
+        if (v.size() != 2) throw dvm::FileIOException::cannotRead(file);
+        xs.push_back(v[0]);
+        zs.push_back(v[1]);
+    }
+    if (xs.size() < 3) throw dvm::FileIOException::cannotRead(file);
+    m_x = Vector(xs);
+    m_z = Vector(zs);
+    std::cout << "Successfully loaded coordinate file with " << m_x.n_elem << " points."
+              << std::endl;
+    m_A = *std::max_element(xs.begin(), xs.end()) - *std::min_element(xs.begin(), xs.end());
+    std::cout << "A = " << m_A << " (assuming cylinder)\n";
+}
+
+void VortexSheet::build_device(uint64_t capacity) {
+    if (m_sim) {
+        dvm_sim_destroy(m_sim);
+        m_sim = nullptr;
+    }
+    const size_t npts = m_x.n_elem, np = npts - 1;
+    m_params.capacity = std::max<uint64_t>(capacity, 1024);
+    m_params.rng_capacity = 2 * m_params.capacity + 64ull * (m_maxNumPanelVort + 1) * np + 4096;
+    dvm::check_status(dvm_sim_create(dvm::device_context(), &m_params, dvm::vec_ptr(m_x),
+                                     dvm::vec_ptr(m_z), (int)npts, &m_sim),
+                      "VortexSheet");
+    // panel geometry, as the reference forms it (src/VortexSheet.cpp:78-102)
+    m_xc.set_size(np);
+    m_zc.set_size(np);
+    m_ds.set_size(np);
+    m_theta.set_size(np);
+    m_enx.set_size(np);
+    m_enz.set_size(np);
+    m_etx.set_size(np);
+    m_etz.set_size(np);
+    dvm::check_status(dvm_sim_get_panels(m_sim, dvm::vec_ptr(m_xc), dvm::vec_ptr(m_zc),
+                                         dvm::vec_ptr(m_ds), dvm::vec_ptr(m_theta),
+                                         dvm::vec_ptr(m_enx), dvm::vec_ptr(m_enz)),
+                      "VortexSheet");
+    for (size_t i = 0; i < np; ++i) {
+        m_etx(i) = -m_enz(i);
+        m_etz(i) = m_enx(i);
+    }
+    if (m_gamma.n_elem != np) {
+        m_gamma.set_size(np);
+        m_gamma.zeros();
+    }
+    dvm::check_status(dvm_sim_set_gamma(m_sim, dvm::vec_ptr(m_gamma)), "VortexSheet");
+}
+
+void VortexSheet::set_params(int precision, int rng, int scheme, int cross, int64_t seed) {
+    m_params.precision = precision;
+    m_params.rng = rng;
+    m_params.scheme = scheme;
+    m_params.surface_cross = cross;
+    m_params.seed = seed;
+    build_device(m_params.capacity);
+}
+
+dvm_sim* VortexSheet::device(uint64_t capacity) {
+    if (!m_sim || capacity > m_params.capacity) build_device(std::max(capacity, 2 * m_params.capacity));
+    return m_sim;
+}
+
+unsigned VortexSheet::max_release() const {
+    return 16u * (m_maxNumPanelVort + 1) * size() + 1024u;
+}
+
+void VortexSheet::upload(VortexBlobs& b) {
+    const unsigned n = b.size();
+    device((uint64_t)n + max_release());
+    dvm::check_status(dvm_sim_set_blobs(m_sim, n, dvm::vec_ptr(b.m_x), dvm::vec_ptr(b.m_z),
+                                        dvm::vec_ptr(b.m_circ), dvm::vec_ptr(b.m_sigma)),
+                      "VortexSheet upload");
+    dvm::check_status(dvm_sim_set_gamma(m_sim, dvm::vec_ptr(m_gamma)), "VortexSheet upload");
+}
+
+void VortexSheet::pull_from_device() {
+    dvm::check_status(dvm_sim_get_gamma(m_sim, dvm::vec_ptr(m_gamma)), "VortexSheet");
+    double cd = 0, cl = 0;
+    dvm::check_status(dvm_sim_get_loads(m_sim, &m_fx, &m_fz, &cd, &cl), "VortexSheet");
+}
+
+void VortexSheet::solvevortexsheet(VortexBlobs& blobs) {
+    upload(blobs);
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_SOLVE), "solvevortexsheet");
+    dvm::check_status(dvm_sim_get_gamma(m_sim, dvm::vec_ptr(m_gamma)), "solvevortexsheet");
+}
+
+void VortexSheet::vortexsheetbc(VortexBlobs& blobs) {
+    upload(blobs);
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_SHEETBC), "vortexsheetbc");
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_get_blobs(m_sim, blobs.size(), &n, nullptr, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr, dvm::vec_ptr(blobs.m_uvs),
+                                        dvm::vec_ptr(blobs.m_wvs), nullptr),
+                      "vortexsheetbc");
+}
+
+VortexBlobs VortexSheet::release_nascent_vortices_rw(Random& rng) {
+    // Run the release on an empty blob set with the next values of the
+    // caller's stream, then consume exactly as many as the release drew.
+    device(max_release());
+    dvm::check_status(dvm_sim_set_blobs(m_sim, 0, nullptr, nullptr, nullptr, nullptr), "release");
+    dvm::check_status(dvm_sim_set_gamma(m_sim, dvm::vec_ptr(m_gamma)), "release");
+    if (m_params.rng == DVM_RNG_INJECT) {
+        std::vector<double> u;
+        rng.peek(max_release(), u);
+        dvm::check_status(dvm_sim_clear_uniforms(m_sim), "release");
+        dvm::check_status(dvm_sim_push_uniforms(m_sim, u.data(), u.size()), "release");
+    }
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_RELEASE), "release_nascent_vortices_rw");
+    dvm::check_status(dvm_sim_status(m_sim), "release_nascent_vortices_rw");
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "release");
+    VortexBlobs nv((unsigned)n);
+    std::vector<uint32_t> ids(n);
+    dvm::check_status(dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(nv.m_x), dvm::vec_ptr(nv.m_z),
+                                        dvm::vec_ptr(nv.m_circ), dvm::vec_ptr(nv.m_sigma),
+                                        dvm::vec_ptr(nv.m_u), dvm::vec_ptr(nv.m_w),
+                                        dvm::vec_ptr(nv.m_uvs), dvm::vec_ptr(nv.m_wvs), ids.data()),
+                      "release");
+    for (uint64_t i = 0; i < n; ++i) nv.m_ID[i] = 0;  // nascent IDs are 0 (src/VortexSheet.cpp:300)
+    if (m_params.rng == DVM_RNG_INJECT) rng.discard(n);  // one draw per nascent blob
+    return nv;
+}
+
+void VortexSheet::reflect(VortexBlobs& v) {
+    upload(v);
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_REFLECT), "reflect");
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_get_blobs(m_sim, v.size(), &n, dvm::vec_ptr(v.m_x),
+                                        dvm::vec_ptr(v.m_z), nullptr, nullptr, nullptr, nullptr,
+                                        nullptr, nullptr, nullptr),
+                      "reflect");
+}
+
+void VortexSheet::delete_inside(VortexBlobs& v) {
+    const unsigned n0 = v.size();
+    upload(v);
+    // keep the velocities too: the reference's compaction copies them
+    std::vector<double> u(v.m_u.memptr(), v.m_u.memptr() + n0), w(v.m_w.memptr(), v.m_w.memptr() + n0);
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_DELETE), "delete_inside");
+    uint64_t n = 0;
+    dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "delete_inside");
+    if (n == n0) return;  // nothing deleted: IDs unchanged (src/VortexSheet.cpp:420-422)
+    VortexBlobs nv((unsigned)n);
+    std::vector<uint32_t> ids(n);
+    dvm::check_status(dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(nv.m_x), dvm::vec_ptr(nv.m_z),
+                                        dvm::vec_ptr(nv.m_circ), dvm::vec_ptr(nv.m_sigma),
+                                        nullptr, nullptr, nullptr, nullptr, ids.data()),
+                      "delete_inside");
+    // u, w, uvs, wvs follow the kept blobs in order (kept = outside the body)
+    size_t k = 0;
+    for (unsigned i = 0; i < n0 && k < n; ++i) {
+        if (v.m_x(i) != nv.m_x(k) || v.m_z(i) != nv.m_z(k)) continue;
+        nv.m_u(k) = v.m_u(i);
+        nv.m_w(k) = v.m_w(i);
+        nv.m_uvs(k) = v.m_uvs(i);
+        nv.m_wvs(k) = v.m_wvs(i);
+        ++k;
+    }
+    for (uint64_t i = 0; i < n; ++i) nv.m_ID[i] = ids[i];
+    nv.copyOutputConfig(v);
+    const unsigned deleted = n0 - (unsigned)n;
+    v = std::move(nv);
+    std::cout << "Deleted " << deleted << " vortices inside body" << std::endl;
+}
+
+void VortexSheet::compute_loads(double Ur) {
+    (void)Ur;  // the device uses |U| from ux, uz: the same value DVMBase passes
+    dvm::check_status(dvm_sim_set_gamma(m_sim, dvm::vec_ptr(m_gamma)), "compute_loads");
+    dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_LOADS), "compute_loads");
+    double cd = 0, cl = 0;
+    dvm::check_status(dvm_sim_get_loads(m_sim, &m_fx, &m_fz, &cd, &cl), "compute_loads");
+    std::cout << "C_D = " << cd << "\t" << "C_L = " << cl << std::endl;
+}
+
+unsigned VortexSheet::size() const {
+    const size_t n = m_gamma.n_elem;
+    if (n != m_xc.n_elem || n != m_zc.n_elem || n + 1 != m_x.n_elem || n + 1 != m_z.n_elem ||
+        n != m_ds.n_elem || n != m_theta.n_elem || n != m_enx.n_elem || n != m_enz.n_elem ||
+        n != m_etx.n_elem || n != m_etz.n_elem)
+        throw dvm::SizeMismatchException("VortexSheet");
+    return static_cast<unsigned>(n);
+}
+
+void VortexSheet::print_collocation() const {
+    for (unsigned i = 0; i < size(); ++i)
+        std::cout << "(xc,zc) = (" << m_xc(i) << "," << m_zc(i) << ")" << std::endl;
+}
+
+void VortexSheet::print_unit_vectors() const {
+    for (unsigned i = 0; i < size(); ++i)
+        std::cout << "For panel No " << i << " the normal vectors are en = (" << m_enx(i) << ","
+                  << m_enz(i) << ") and et = (" << m_etx(i) << "," << m_etz(i) << ")" << std::endl;
+}
+
+void VortexSheet::print_gamma() const {
+    for (size_t i = 0; i < m_gamma.n_elem; ++i) std::cout << "   " << m_gamma(i) << "\n";
+}
+
+void VortexSheet::write_step(double time) {
+    // formats of src/VortexSheet.cpp:335-343
+    for (size_t i = 0; i < m_xc.n_elem; ++i)
+        m_gammafile << time << "\t " << m_xc(i) << "\t" << m_zc(i) << "\t" << m_gamma(i) << "\t"
+                    << m_ds(i) << "\n";
+    m_forcefile << time << "\t" << m_fx << "\t" << m_fz << "\n";
+}
+
+std::tuple<double, double> VortexSheet::get_forces() const { return std::make_tuple(m_fx, m_fz); }
+
+void VortexSheet::probe_velocities(const VortexBlobs&, Probe&) {
+    throw dvm::AlgorithmException("VortexSheet::probe_velocities is not provided by this build");
+}

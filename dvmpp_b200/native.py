@@ -396,6 +396,10 @@ class ServerSummary(C.Structure):
 
 SIGNATURES.update({
     "dvm_ctx_reserve": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int]),
+    "dvm_random_walk": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, C.c_double, C.c_double]),
+    "dvm_sim_set_step": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "dvm_sim_clear_uniforms": (C.c_int, [C.c_void_p]),
+    "dvm_sim_pending_uniforms": (C.c_int, [C.c_void_p, _dp, C.c_uint64, C.POINTER(C.c_uint64)]),
     "dvm_ctx_workspace_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "dvm_server_create": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "dvm_server_destroy": (C.c_int, [C.c_void_p]),

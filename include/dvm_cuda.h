@@ -170,6 +170,12 @@ int dvm_biot_savart_at_device(dvm_ctx* ctx, const double* x, const double* z, co
                               const double* tz, uint64_t nt, double* u, double* w,
                               int precision, int skip_close);
 
+/* Random walk of a host blob set with host uniforms R (2n values, R1 R2 per
+ * blob in blob order): VortexBlobs::diffusion_random_walk,
+ * src/VortexBlobs.cpp:251-265.  x and z are updated in place. */
+int dvm_random_walk(dvm_ctx* ctx, double* x, double* z, uint64_t n, const double* R, double nu,
+                    double dt);
+
 /* Velocity at targets without any device allocation.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: code whose device memory is owned by a host framework's
@@ -216,9 +222,14 @@ int dvm_sim_get_panels(dvm_sim* sim, double* xc, double* zc, double* ds, double*
                        double* enx, double* enz);
 int dvm_sim_get_loads(dvm_sim* sim, double* fx, double* fz, double* cd, double* cl);
 int dvm_sim_get_step(dvm_sim* sim, uint32_t* step);
+int dvm_sim_set_step(dvm_sim* sim, uint32_t step);
 /* Inject mode: append uniforms in (0,1) to the device stream (in draw order). */
 int dvm_sim_push_uniforms(dvm_sim* sim, const double* u, uint64_t n);
 int dvm_sim_rng_position(dvm_sim* sim, uint64_t* consumed_total, uint64_t* available);
+/* Inject mode: drop the uniforms still held on the device. */
+int dvm_sim_clear_uniforms(dvm_sim* sim);
+/* Inject mode: copy out the uniforms pushed but not yet consumed (in order). */
+int dvm_sim_pending_uniforms(dvm_sim* sim, double* out, uint64_t cap, uint64_t* n);
 /* First error raised on the device for this simulation (synchronises). */
 int dvm_sim_status(dvm_sim* sim);
 int dvm_sim_clear_status(dvm_sim* sim);

@@ -348,6 +348,7 @@ class Ref:
         L.ref_sim_phase.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.ref_sim_nblobs.argtypes = [C.c_void_p]
         L.ref_sim_nblobs.restype = C.c_size_t
+        L.ref_sim_write.argtypes = [C.c_void_p]
         L.ref_sim_npanels.argtypes = [C.c_void_p]
         L.ref_sim_get_blobs.argtypes = [C.c_void_p] + [_dp] * 8 + [_up]
         L.ref_sim_set_blobs.argtypes = [C.c_void_p, C.c_size_t] + [_dp] * 4
@@ -414,6 +415,10 @@ class RefSim:
 
     def phase(self, k):
         if self.L.ref_sim_phase(self.h, k, self.quiet):
+            raise RuntimeError(self.ref.err())
+
+    def write_outputs(self):
+        if self.L.ref_sim_write(self.h):
             raise RuntimeError(self.ref.err())
 
     @property

@@ -176,6 +176,17 @@ int ref_sim_phase(void* h, int phase, int quiet) {
     }
 }
 
+// DVMBase::write_outputs (src/DVMBase.cpp:151-158): the per-step text files.
+int ref_sim_write(void* h) {
+    try {
+        static_cast<RefSim*>(h)->base->write_outputs();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 size_t ref_sim_nblobs(void* h) { return static_cast<RefSim*>(h)->base->m_vortex.size(); }
 int ref_sim_npanels(void* h) { return static_cast<int>(static_cast<RefSim*>(h)->base->m_vortsheet.size()); }
 
