@@ -249,14 +249,20 @@ def ref_sample_step(ref, inst, workdir):
     return t
 
 
-def reference_sample(instances, n_samples: int):
+def reference_sample(instances, n_samples: int, spread: bool = False):
+    """Run one reference compute_step on n_samples instances (the smallest, or
+    with spread=True, instances at evenly spaced size quantiles up to the
+    median) and extrapolate the per-phase rates to the whole batch."""
     from oracle.pyoracle import Ref, have_ref
 
     if not have_ref():
         return None
     ref = Ref()
     order = sorted(range(len(instances)), key=lambda k: instances[k]["nblobs"])
-    pick = order[:n_samples]
+    if spread:
+        pick = [order[(len(order) // 2) * j // max(n_samples - 1, 1)] for j in range(n_samples)]
+    else:
+        pick = order[:n_samples]
     model = RefModel()
     total = 0.0
     with tempfile.TemporaryDirectory(prefix="dvmref_") as wd:
@@ -356,10 +362,12 @@ def run_ours(args, dist):
     ctx.sync()
     clocks.start()
     l0 = ctx.launches()
+    ctx.profiler_range(True)  # an external profiler run with collection off sees only this
     ctx.mark(0)
     ctx.step_batch(sims, args.steps, use_graph=True)
     ctx.mark(1)
     ms = ctx.elapsed_ms(0, 1)
+    ctx.profiler_range(False)
     launches = ctx.launches() - l0
     clock_info = clocks.stop()
     for s in sims:
@@ -436,12 +444,12 @@ def run_ours(args, dist):
     # ---- CPU baseline (rank 0, N = 1): the reference itself, bounded sample
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        r = reference_sample(instances, 2)
+        r = reference_sample(instances, 3, spread=True)
         if r:
             cpu = {"value": args.instances / r["batch_step_s"], "unit": UNIT, "cores": _cores(),
                    "kind": "reference",
-                   "sample": f"one reference compute_step (phase-timed) on each of the 2 "
-                             f"smallest instances (N={r['sampled']}), per-phase rates "
+                   "sample": f"one reference compute_step (phase-timed) on each of 3 "
+                             f"instances from the smallest to the median (N={r['sampled']}), per-phase rates "
                              f"extrapolated to all {args.instances} instances; output writing "
                              f"off; {r['wall_s']:.1f} s of CPU work"}
 
@@ -481,11 +489,37 @@ def run_ours(args, dist):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
-    if dist.rank == 0:
-        print(json.dumps(line))
     for s in sims:
         s.close()
     ctx.close()
+
+    # ---- the standalone N-body configuration (N = 2^20 wake) and the serving
+    # loop (continuous batching vs the plain serial path): reported beside
+    if args.nbody_n:
+        from dvmpp_b200 import cases
+
+        nb = cases.run_nbody(args.nbody_n, [N.F32], 2)
+        r = nb["results"]["f32"]
+        line["nbody"] = {"n": args.nbody_n, "pair_kernel_ms": r["pair_kernel_ms"],
+                         "gpairs_per_s": r["gpairs_per_s"], "tflops_12_per_pair": r["tflops_12_per_pair"],
+                         "fp32_peak_frac": r["fp32_peak_frac"]}
+    if args.serve_requests:
+        from dvmpp_b200 import cases
+
+        sv = cases.run_serving(args.serve_requests, 7, 20.0, (20, 100), (64, 512), 256, 100.0,
+                               True, True)
+        b, s = sv["batched"], sv["serial"]
+        line["serving"] = {
+            "requests": args.serve_requests, "arrivals": "Poisson 20 req/s (seed 7), realtime",
+            "steps": "U{20..100} (scaled from U{100..2000})", "panels": "U{64..512}",
+            "sim_steps_per_s": b["sim_steps_per_s"], "serial_sim_steps_per_s": s["sim_steps_per_s"],
+            "ratio_batched_over_serial": sv["speedup_sim_steps"],
+            "latency_p50_s": b["latency_p50_s"], "latency_p95_s": b["latency_p95_s"],
+            "latency_p99_s": b["latency_p99_s"], "serial_latency_p50_s": s["latency_p50_s"],
+            "serial_latency_p99_s": s["latency_p99_s"], "peak_active": b["peak_active"],
+            "peak_bytes": b["peak_bytes"]}
+    if dist.rank == 0:
+        print(json.dumps(line))
 
 
 def main(argv=None):
@@ -500,6 +534,10 @@ def main(argv=None):
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nbody-n", type=int, default=1 << 20,
+                    help="standalone N-body leg size (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="serving leg request count (0: skip)")
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per pair-kernel launch from an ncu capture")
     args = ap.parse_args(argv)

@@ -16,6 +16,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_profiler_api.h>
+
 #include "../../include/dvm_cuda.h"
 #include "dvm_internal.h"
 
@@ -671,6 +673,13 @@ int dvm_ctx_elapsed(dvm_ctx* c, int a, int b, double* ms) {
     float f = 0.f;
     CK(cudaEventElapsedTime(&f, c->marks[a], c->marks[b]));
     *ms = f;
+    return DVM_OK;
+}
+
+int dvm_ctx_profiler_range(dvm_ctx* c, int on) {
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    CK(cudaSetDevice(c->device));
+    CK(on ? cudaProfilerStart() : cudaProfilerStop());
     return DVM_OK;
 }
 

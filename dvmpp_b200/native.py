@@ -69,6 +69,7 @@ SIGNATURES = {
     "dvm_ctx_mark": (C.c_int, [C.c_void_p, C.c_int]),
     "dvm_ctx_elapsed": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _dp]),
     "dvm_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "dvm_ctx_profiler_range": (C.c_int, [C.c_void_p, C.c_int]),
     "dvm_ctx_profile": (C.c_int, [C.c_void_p, C.c_int, _dp, C.POINTER(C.c_uint64)]),
     "dvm_ctx_profile_reset": (C.c_int, [C.c_void_p]),
     "dvm_biot_savart_self": (C.c_int, [C.c_void_p, C.POINTER(Particle), C.c_uint64, C.POINTER(Velocity), C.c_int]),
@@ -176,6 +177,9 @@ class Context:
         v = C.c_double()
         _check(self.lib.dvm_ctx_elapsed(self.h, a, b, C.byref(v)))
         return v.value
+
+    def profiler_range(self, on: bool):
+        _check(self.lib.dvm_ctx_profiler_range(self.h, 1 if on else 0))
 
     def set_profiling(self, on: bool):
         _check(self.lib.dvm_ctx_set_profiling(self.h, 1 if on else 0))

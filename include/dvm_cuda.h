@@ -150,6 +150,9 @@ int dvm_ctx_workspace_bytes(dvm_ctx* ctx, uint64_t* bytes);
 int dvm_ctx_mark(dvm_ctx* ctx, int slot);
 int dvm_ctx_elapsed(dvm_ctx* ctx, int slot_a, int slot_b, double* ms);
 int dvm_ctx_set_profiling(dvm_ctx* ctx, int on);
+/* Bracket a region for an external profiler started with collection off
+ * (cudaProfilerStart / cudaProfilerStop); harmless without one. */
+int dvm_ctx_profiler_range(dvm_ctx* ctx, int on);
 int dvm_ctx_profile(dvm_ctx* ctx, int family, double* ms_total, uint64_t* launches);
 int dvm_ctx_profile_reset(dvm_ctx* ctx);
 /* Bytes a simulation with these parameters and np panels occupies. */
