@@ -320,6 +320,19 @@ def run_reference_arm(args, dist):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def committed_traffic():
+    """DRAM bytes per pair-kernel launch on this workload, from the committed
+    ncu summary (one capture of the first timed step)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "bench_batched64_launches.md")) as f:
+            for ln in f:
+                if ln.strip().startswith("dram_bytes_per_launch:"):
+                    return float(ln.split(":")[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -473,7 +486,11 @@ def run_ours(args, dist):
                       "how": "each simulation stepped alone (its own launches, no batching)"},
         "roofline": {"bound": "fp32", "kernel": "k_self_f32 (pair kernel)",
                      "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved_tflops / fp32_peak, "traffic": args.traffic,
+                     "frac": achieved_tflops / fp32_peak,
+                     "traffic": args.traffic if args.traffic is not None else committed_traffic(),
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one "
+                                       "launch of this workload (profiles/"
+                                       "bench_batched64_launches.md)",
                      "flops_per_pair": 12, "pairs_per_launch": pairs_per_launch,
                      "launch_ms": nbody_launch_ms,
                      "peak_source": f"derived: {sms} SMs x 128 FP32 lanes x 2 x "
@@ -482,6 +499,9 @@ def run_ours(args, dist):
                      "share_of_step": nb_ms / max(prof["step"][0], 1e-9)},
         "profile_ms_per_step": {k: v[0] / max(args.prof_steps, 1) for k, v in prof.items()},
         "gpu_launches": int(launches),
+        "gpu_launches_note": "own kernels in the timed region; each step's Morton sort adds "
+                             "the CUB radix-sort kernels compiled into the same library "
+                             "(7 per step in the ncu launch list)",
         "clocks": clock_info,
         "setup_s": setup_s,
     }
