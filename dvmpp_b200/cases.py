@@ -8,12 +8,23 @@ Gamma ~ N(0, 1e-3) summing to zero, sigma = 0.081880 (ds^0.675 of the
 128-panel R = 0.5 circle), seed 2.  Prints one JSON line with the pair
 kernel's CUDA-event time, pairs/s, FP32-pipe fraction and (with both
 precisions) the FP32-vs-FP64 error.
+
+    python -m dvmpp_b200.cases precision [--steps 20] [--n-wake 524288] [--panels 1024]
+
+precision: ellipse (0.5, 0.25) at 20 degrees, 1024 panels (a 1025 x 1024
+influence matrix), a 2^19-blob wake, RK3 dt = 0.002; the FP32-compensated run
+(FP64 QR, FP64 refinement and Kelvin row) against an all-FP64 run.
+
+    python -m dvmpp_b200.cases serve [--requests 100] [--serial] [--realtime]
+
+serve: the continuous-batching server on Poisson arrivals (seed 7, 20 req/s).
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import time
 
 import numpy as np
 
@@ -107,6 +118,92 @@ def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, m
     return out
 
 
+def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
+                  incidence_deg: float = 20.0):
+    """Sheet-solve precision: an ellipse (semi-axes 0.5, 0.25) at the given
+    incidence, npanels panels, a wake of n_wake blobs (the N-body distribution,
+    core size ds^0.675 of this body), RK3 with dt = 0.002, nu = 1e-3, ux = 1.
+    One run with FP32 compensated pair sums (FP64 QR + FP64 refinement,
+    Kelvin row in FP64) beside an all-FP64 run from the same state and the
+    same Philox stream.  Reports per-step gamma / Cd / Cl differences, the
+    blob counts, the least-squares solvers against each other on one right-
+    hand side, and the velocity fields of both precisions evaluated on one
+    identical final state."""
+    M = 3
+    ctx = N.Context(0)
+    bx, bz = W.ellipse(npanels, 0.5, 0.25, incidence_deg)
+    ds = np.hypot(np.diff(bx), np.diff(bz))
+    sigma = float(np.mean(ds)) ** 0.675
+    x, z, g, s = W.wake(n_wake, seed, sigma)
+    cap = n_wake + (steps + 2) * (M + 1) * npanels + 4096
+    common = dict(rho=1.0, nu=1e-3, dt=0.002, ux=1.0, uz=0.0, max_numpanelvort=M,
+                  scheme=N.RK3, surface_cross=N.REFLECT, rng=N.RNG_PHILOX, seed=11,
+                  capacity=cap)
+    sims = {name: ctx.sim(N.Params(precision=prec, **common), bx, bz)
+            for name, prec in (("f32", N.F32), ("f64", N.F64))}
+    for sim in sims.values():
+        sim.set_blobs(x, z, g, s)
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    mx = lambda a, b: float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+    # least-squares solvers on one right-hand side (the initial wake's)
+    s64 = sims["f64"]
+    s64.phase(N.PHASE_SOLVE)
+    A, b, g_qr = s64.influence(), s64.rhs(), s64.gamma()
+    g_ls = np.linalg.lstsq(A, b, rcond=None)[0]
+    g_ne = np.linalg.solve(A.T @ A, A.T @ b)
+    sims["f32"].phase(N.PHASE_SOLVE)
+    solve = {"matrix": list(A.shape), "cond_A": float(np.linalg.cond(A)),
+             "qr_refined_vs_lstsq": rel(g_qr, g_ls),
+             "normal_equations_vs_lstsq": rel(g_ne, g_ls),
+             "f32_rhs_qr_refined_vs_f64": rel(sims["f32"].gamma(), g_qr),
+             "residual_norm_qr": float(np.linalg.norm(A @ g_qr - b)),
+             "residual_norm_lstsq": float(np.linalg.norm(A @ g_ls - b))}
+
+    rows = []
+    t = {"f32": 0.0, "f64": 0.0}
+    for k in range(steps):
+        for name, sim in sims.items():
+            ctx.sync()
+            t0 = time.perf_counter()
+            sim.step(1)
+            ctx.sync()
+            t[name] += time.perf_counter() - t0
+            sim.check()
+        l32, l64 = sims["f32"].loads(), sims["f64"].loads()
+        rows.append({"step": k + 1, "n_f32": sims["f32"].n, "n_f64": sims["f64"].n,
+                     "gamma_rel_l2": rel(sims["f32"].gamma(), sims["f64"].gamma()),
+                     "cd_f32": l32[2], "cd_f64": l64[2], "cl_f32": l32[3], "cl_f64": l64[3]})
+
+    # both precisions evaluated on one identical state (the FP64 run's final one)
+    d64 = sims["f64"].blobs()
+    sims["f32"].set_blobs(d64["x"], d64["z"], d64["circ"], d64["sigma"])
+    fields = {}
+    for name, sim in sims.items():
+        for ph in (N.PHASE_BIOTSAVART, N.PHASE_SOLVE, N.PHASE_SHEETBC):
+            sim.phase(ph)
+        d = sim.blobs()
+        fields[name] = (d, sim.gamma())
+    (d32, g32), (dd, gd) = fields["f32"], fields["f64"]
+    same_state = {"n": int(dd["x"].size), "gamma_rel_l2": rel(g32, gd), "gamma_max": mx(g32, gd)}
+    for key in ("u", "w", "uvs", "wvs"):
+        same_state[key + "_rel_l2"] = rel(d32[key], dd[key])
+        same_state[key + "_max"] = mx(d32[key], dd[key])
+    ctx.close()
+    cd_err = max(abs(r["cd_f32"] - r["cd_f64"]) / max(abs(r["cd_f64"]), 1e-12) for r in rows)
+    cl_err = max(abs(r["cl_f32"] - r["cl_f64"]) for r in rows)
+    return {"workload": "precision", "npanels": npanels, "incidence_deg": incidence_deg,
+            "n_wake": n_wake, "sigma": sigma, "steps": steps, "scheme": "RK3", "dt": 0.002,
+            "solve": solve, "same_state": same_state,
+            "run": {"steps_with_equal_n": sum(r["n_f32"] == r["n_f64"] for r in rows),
+                    "max_gamma_rel_l2": max(r["gamma_rel_l2"] for r in rows),
+                    "max_cd_rel": cd_err, "max_cl_abs": cl_err,
+                    "final": rows[-1] if rows else None,
+                    "s_per_step_f32": t["f32"] / max(steps, 1),
+                    "s_per_step_f64": t["f64"] / max(steps, 1)},
+            "per_step": rows}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -127,7 +224,14 @@ def main(argv=None):
     sv.add_argument("--serial", action="store_true", help="also run the plain serial path")
     sv.add_argument("--no-graph", action="store_true")
     sv.add_argument("--no-sync", action="store_true")
+    pr = sub.add_parser("precision")
+    pr.add_argument("--steps", type=int, default=20)
+    pr.add_argument("--n-wake", type=int, default=1 << 19)
+    pr.add_argument("--panels", type=int, default=1024)
+    pr.add_argument("--seed", type=int, default=2)
     a = ap.parse_args(argv)
+    if a.cmd == "precision":
+        print(json.dumps(run_precision(a.steps, a.n_wake, a.panels, a.seed)))
     if a.cmd == "serve":
         print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
                                      a.max_active, a.budget_gb, a.realtime, a.serial,

@@ -3,9 +3,11 @@
 // velocity fused with the convection update (src/VortexSheet.cpp:217-273,
 // src/DVMBase.cpp:167-209) and the pressure loads (src/VortexSheet.cpp:487-514).
 //
-// All FP64.  Pair formulas keep the reference's operation order with one
+// FP64 instances: pair formulas keep the reference's operation order with one
 // rounding per operation (dadd/dmul/...), so they round like the reference
-// compiled without FP contraction.
+// compiled without FP contraction.  FP32 instances evaluate the sheet-on-blob
+// panel terms in single precision (accumulated in FP64); the influence matrix,
+// QR, solve, refinement and loads are FP64 for both.
 //
 // The solve: the reference forms A^T A and A^T b and solves with LAPACK every
 // call.  Here A ((np+1) x np) is factorised ONCE per body by Householder QR on
@@ -179,12 +181,42 @@ __global__ void k_residual(const InstDesc* __restrict__ table, const ListEntry* 
 }
 
 // ---- sheet-on-blob velocity (+ convection) -------------------------------------
+// One panel term of src/VortexSheet.cpp:235-249 in FP32 for the FP32-precision
+// instances.  The blob offset from the collocation point is formed in FP64
+// and rounded once; log(1 + x) and atan2 are the accurate single-precision
+// library functions.  The contribution px g0 + qx g1 is evaluated as
+// (px + qx) g0 + qx (g1 - g0): px + qx = -c6/2 sin - c7 cos has no
+// cancellation, whereas px and qx separately are O(1) terms that cancel to
+// O(ds / r) for distant blobs, so this grouping keeps FP32 rounding relative
+// to the result (the FP64 instances keep the reference's grouping).
+struct PanelF32 {
+    float ct, st, ds, ids, c2, s2;
+};
+
+__device__ __forceinline__ void sheet_pair_f32(float dx, float dz, const PanelF32& P, float g0,
+                                               float dg, double& us, double& ws) {
+    const float c1 = -dx * P.ct - dz * P.st;
+    const float c2 = fmaf(dx, dx, dz * dz);
+    const float c5 = dx * P.st - dz * P.ct;
+    const float c6 = log1pf(__fdividef(P.ds * fmaf(2.0f, c1, P.ds), c2));
+    const float c7 = atan2f(c5 * P.ds, fmaf(c1, P.ds, c2));
+    const float c8 = dx * P.s2 + dz * P.c2;
+    const float c9 = dx * P.c2 - dz * P.s2;
+    const float h6 = 0.5f * c6 * P.ids, c7i = c7 * P.ids;
+    const float qx = -P.st + c8 * h6 + (c1 * P.ct + c5 * P.st) * c7i;
+    const float qy = P.ct + c9 * h6 + (c1 * P.st - c5 * P.ct) * c7i;
+    const float ax = -0.5f * c6 * P.st - c7 * P.ct;  // px + qx
+    const float ay = 0.5f * c6 * P.ct - c7 * P.st;   // py + qy
+    us += (double)fmaf(ax, g0, qx * dg);
+    ws += (double)fmaf(ay, g0, qy * dg);
+}
+
 __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restrict__ table,
                                                         const InstState* __restrict__ st,
                                                         const ListEntry* __restrict__ list,
                                                         int nlist, int mode,
                                                         unsigned* __restrict__ work) {
-    extern __shared__ double s_pan[];  // 8 arrays of max_np
+    extern __shared__ double s_pan[];  // FP64: 8 arrays of max_np; FP32: see below
     __shared__ unsigned s_pre[1025];
     __shared__ unsigned s_item;
     __shared__ int s_loaded;
@@ -208,6 +240,7 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         const ListEntry e = list[k];
         const InstDesc& d = table[e.inst];
         const int np = d.np;
+        const bool f32 = d.precision == kF32;
         double* sxc = s_pan;
         double* szc = sxc + np;
         double* sds = szc + np;
@@ -216,16 +249,30 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         double* sc2 = sst + np;
         double* ss2 = sc2 + np;
         double* sg = ss2 + np;
+        // FP32 layout after xc, zc: np PanelF32 records, then np gamma_j and
+        // np (gamma_{j+1} - gamma_j) (wrapping at the last panel)
+        PanelF32* fpan = reinterpret_cast<PanelF32*>(szc + np);
+        float* fg = reinterpret_cast<float*>(fpan + np);
+        float* fdg = fg + np;
         if (s_loaded != k) {
             for (int j = threadIdx.x; j < np; j += blockDim.x) {
                 sxc[j] = d.xc[j];
                 szc[j] = d.zc[j];
-                sds[j] = d.ds[j];
-                sct[j] = d.cth[j];
-                sst[j] = d.sth[j];
-                sc2[j] = d.c2th[j];
-                ss2[j] = d.s2th[j];
-                sg[j] = d.gamma[j];
+                if (f32) {
+                    const double dsj = d.ds[j];
+                    fpan[j] = PanelF32{(float)d.cth[j], (float)d.sth[j], (float)dsj,
+                                       (float)(1.0 / dsj), (float)d.c2th[j], (float)d.s2th[j]};
+                    const double g0 = d.gamma[j], g1 = d.gamma[j == np - 1 ? 0 : j + 1];
+                    fg[j] = (float)g0;
+                    fdg[j] = (float)(g1 - g0);
+                } else {
+                    sds[j] = d.ds[j];
+                    sct[j] = d.cth[j];
+                    sst[j] = d.sth[j];
+                    sc2[j] = d.c2th[j];
+                    ss2[j] = d.s2th[j];
+                    sg[j] = d.gamma[j];
+                }
             }
         }
         __syncthreads();
@@ -235,25 +282,32 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         if (i < n) {
             const double xi = d.x[i], zi = d.z[i];
             double us = 0.0, ws = 0.0;
-            for (int j = 0; j < np; ++j) {
-                const double dsj = sds[j], ct = sct[j], stt = sst[j];
-                const double dx = dsub(xi, sxc[j]), dz = dsub(zi, szc[j]);
-                const double c1 = dsub(dmul(-dx, ct), dmul(dz, stt));
-                const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
-                const double c5 = dsub(dmul(dx, stt), dmul(dz, ct));
-                const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
-                const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
-                const double c8 = dadd(dmul(dx, ss2[j]), dmul(dz, sc2[j]));
-                const double c9 = dsub(dmul(dx, sc2[j]), dmul(dz, ss2[j]));
-                const double qx = dadd(dadd(-stt, ddiv(dmul(dmul(0.5, c8), c6), dsj)),
-                                       ddiv(dmul(dadd(dmul(c1, ct), dmul(c5, stt)), c7), dsj));
-                const double px = dsub(dsub(dmul(dmul(-0.5, c6), stt), dmul(c7, ct)), qx);
-                const double qy = dadd(dadd(ct, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
-                                       ddiv(dmul(dsub(dmul(c1, stt), dmul(c5, ct)), c7), dsj));
-                const double py = dsub(dsub(dmul(dmul(0.5, c6), ct), dmul(c7, stt)), qy);
-                const double g0 = sg[j], g1 = (j == np - 1) ? sg[0] : sg[j + 1];
-                us = dadd(us, dadd(dmul(px, g0), dmul(qx, g1)));
-                ws = dadd(ws, dadd(dmul(py, g0), dmul(qy, g1)));
+            if (f32) {
+#pragma unroll 2
+                for (int j = 0; j < np; ++j)
+                    sheet_pair_f32((float)(xi - sxc[j]), (float)(zi - szc[j]), fpan[j], fg[j],
+                                   fdg[j], us, ws);
+            } else {
+                for (int j = 0; j < np; ++j) {
+                    const double dsj = sds[j], ct = sct[j], stt = sst[j];
+                    const double dx = dsub(xi, sxc[j]), dz = dsub(zi, szc[j]);
+                    const double c1 = dsub(dmul(-dx, ct), dmul(dz, stt));
+                    const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
+                    const double c5 = dsub(dmul(dx, stt), dmul(dz, ct));
+                    const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
+                    const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
+                    const double c8 = dadd(dmul(dx, ss2[j]), dmul(dz, sc2[j]));
+                    const double c9 = dsub(dmul(dx, sc2[j]), dmul(dz, ss2[j]));
+                    const double qx = dadd(dadd(-stt, ddiv(dmul(dmul(0.5, c8), c6), dsj)),
+                                           ddiv(dmul(dadd(dmul(c1, ct), dmul(c5, stt)), c7), dsj));
+                    const double px = dsub(dsub(dmul(dmul(-0.5, c6), stt), dmul(c7, ct)), qx);
+                    const double qy = dadd(dadd(ct, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
+                                           ddiv(dmul(dsub(dmul(c1, stt), dmul(c5, ct)), c7), dsj));
+                    const double py = dsub(dsub(dmul(dmul(0.5, c6), ct), dmul(c7, stt)), qy);
+                    const double g0 = sg[j], g1 = (j == np - 1) ? sg[0] : sg[j + 1];
+                    us = dadd(us, dadd(dmul(px, g0), dmul(qx, g1)));
+                    ws = dadd(ws, dadd(dmul(py, g0), dmul(qy, g1)));
+                }
             }
             const double uvs = dmul(us, kRpi2), wvs = dmul(ws, kRpi2);
             d.uvs[i] = uvs;

@@ -75,12 +75,14 @@ def test_sheet_solve_and_velocity(ctx, port, prec):
     assert close(b, b0, 1e-12 if prec == N.F64 else 2e-6)
     gam = s.gamma()
     assert close(gam, g0, 1e-9 if prec == N.F64 else 5e-5)
-    # sheet-on-blob from the oracle's gamma on both sides
+    # sheet-on-blob from the oracle's gamma on both sides (FP32 instances
+    # evaluate the panel terms in single precision: max error <= 1e-5 of max)
     s.set_gamma(g0)
     s.phase(N.PHASE_SHEETBC)
     uvs0, wvs0 = port.sheet_on_blobs(geo, g0, x, z)
     d = s.blobs()
-    assert close(d["uvs"], uvs0, 1e-12) and close(d["wvs"], wvs0, 1e-12)
+    tol = 1e-12 if prec == N.F64 else 1e-5
+    assert close(d["uvs"], uvs0, tol) and close(d["wvs"], wvs0, tol)
     s.close()
 
 
