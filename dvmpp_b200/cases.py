@@ -183,20 +183,30 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
         for ph in (N.PHASE_BIOTSAVART, N.PHASE_SOLVE, N.PHASE_SHEETBC):
             sim.phase(ph)
         d = sim.blobs()
-        fields[name] = (d, sim.gamma())
-    (d32, g32), (dd, gd) = fields["f32"], fields["f64"]
-    same_state = {"n": int(dd["x"].size), "gamma_rel_l2": rel(g32, gd), "gamma_max": mx(g32, gd)}
+        fields[name] = (d, sim.gamma(), sim.rhs())
+    (d32, g32, b32), (dd, gd, bd) = fields["f32"], fields["f64"]
+    same_state = {"n": int(dd["x"].size), "gamma_rel_l2": rel(g32, gd), "gamma_max": mx(g32, gd),
+                  "rhs_rel_l2": rel(b32[:-1], bd[:-1]), "rhs_max": mx(b32[:-1], bd[:-1]),
+                  "kelvin_row_abs": float(abs(b32[-1] - bd[-1]))}
     for key in ("u", "w", "uvs", "wvs"):
         same_state[key + "_rel_l2"] = rel(d32[key], dd[key])
         same_state[key + "_max"] = mx(d32[key], dd[key])
+    # the FP32 sheet-on-blob kernel alone: both evaluate with the FP64 gamma
+    sims["f32"].set_gamma(gd)
+    sims["f32"].phase(N.PHASE_SHEETBC)
+    ds32 = sims["f32"].blobs()
+    for key in ("uvs", "wvs"):
+        same_state[key + "_same_gamma_rel_l2"] = rel(ds32[key], dd[key])
+        same_state[key + "_same_gamma_max"] = mx(ds32[key], dd[key])
     ctx.close()
-    cd_err = max(abs(r["cd_f32"] - r["cd_f64"]) / max(abs(r["cd_f64"]), 1e-12) for r in rows)
-    cl_err = max(abs(r["cl_f32"] - r["cl_f64"]) for r in rows)
+    cd_err = max((abs(r["cd_f32"] - r["cd_f64"]) / max(abs(r["cd_f64"]), 1e-12) for r in rows),
+                 default=0.0)
+    cl_err = max((abs(r["cl_f32"] - r["cl_f64"]) for r in rows), default=0.0)
     return {"workload": "precision", "npanels": npanels, "incidence_deg": incidence_deg,
             "n_wake": n_wake, "sigma": sigma, "steps": steps, "scheme": "RK3", "dt": 0.002,
             "solve": solve, "same_state": same_state,
             "run": {"steps_with_equal_n": sum(r["n_f32"] == r["n_f64"] for r in rows),
-                    "max_gamma_rel_l2": max(r["gamma_rel_l2"] for r in rows),
+                    "max_gamma_rel_l2": max((r["gamma_rel_l2"] for r in rows), default=0.0),
                     "max_cd_rel": cd_err, "max_cl_abs": cl_err,
                     "final": rows[-1] if rows else None,
                     "s_per_step_f32": t["f32"] / max(steps, 1),

@@ -565,7 +565,7 @@ __global__ void k_self_combine(const InstDesc* __restrict__ table,
 // ---- arbitrary targets --------------------------------------------------------
 // One item = (entry, 256 targets, kAtChunk sources).  Sources are staged with
 // FP64 positions; each pair forms dx, dz in FP64 (exact for close pairs) and,
-// in FP32 mode, evaluates the kernel in FP32 with a Kahan fold per stage.
+// in FP32 mode, evaluates the kernel in FP32 with Kahan-compensated sums.
 struct AtJob {
     const double* tx;
     const double* tz;
@@ -626,7 +626,9 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
             __syncthreads();
             const int cnt = (int)min(256u, j1 - s0);
             if (F32) {
-                float pu = 0.f, pw = 0.f;
+                // compensated per pair: the right-hand side is the small
+                // residual normal velocity, so the sum's rounding must stay
+                // relative to the few large near-blob terms, not compound
                 for (int jj = 0; jj < cnt; ++jj) {
                     const float dx = (float)(tx - s_x[jj]);
                     const float dz = (float)(tz - s_z[jj]);
@@ -635,16 +637,9 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                     float K = rcp_approx(r2);
                     if (r2 < (float)s_thr[jj]) K = core_kernel(r2, (float)s_rs[jj], K);
                     const float g = K * (float)s_c[jj];
-                    pu = fmaf(-g, dz, pu);
-                    pw = fmaf(g, dx, pw);
+                    kahan(su, cu, -g * dz);
+                    kahan(sw, cw, g * dx);
                 }
-                float y = pu - cu, tt = su + y;
-                cu = (tt - su) - y;
-                su = tt;
-                y = pw - cw;
-                tt = sw + y;
-                cw = (tt - sw) - y;
-                sw = tt;
             } else {
                 for (int jj = 0; jj < cnt; ++jj) {
                     const double dx = dsub(tx, s_x[jj]);

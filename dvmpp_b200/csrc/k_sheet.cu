@@ -182,9 +182,12 @@ __global__ void k_residual(const InstDesc* __restrict__ table, const ListEntry* 
 
 // ---- sheet-on-blob velocity (+ convection) -------------------------------------
 // One panel term of src/VortexSheet.cpp:235-249 in FP32 for the FP32-precision
-// instances.  The blob offset from the collocation point is formed in FP64
-// and rounded once; log(1 + x) and atan2 are the accurate single-precision
-// library functions.  The contribution px g0 + qx g1 is evaluated as
+// instances.  The blob's offsets from the panel's start (the collocation
+// point) and end are formed in FP64 and rounded once.  c6 = log(|p-e|^2 /
+// |p-s|^2) is taken as log1p(x), x = ds (ds + 2 c1) / c2, while |x| < 1/2,
+// and as the log of the two squared distances' ratio otherwise, so a blob
+// next to the panel's end (nascent blobs sit there) keeps full relative
+// accuracy.  The contribution px g0 + qx g1 is evaluated as
 // (px + qx) g0 + qx (g1 - g0): px + qx = -c6/2 sin - c7 cos has no
 // cancellation, whereas px and qx separately are O(1) terms that cancel to
 // O(ds / r) for distant blobs, so this grouping keeps FP32 rounding relative
@@ -193,12 +196,15 @@ struct PanelF32 {
     float ct, st, ds, ids, c2, s2;
 };
 
-__device__ __forceinline__ void sheet_pair_f32(float dx, float dz, const PanelF32& P, float g0,
-                                               float dg, double& us, double& ws) {
+__device__ __forceinline__ void sheet_pair_f32(float dx, float dz, float dxe, float dze,
+                                               const PanelF32& P, float g0, float dg, double& us,
+                                               double& ws) {
     const float c1 = -dx * P.ct - dz * P.st;
     const float c2 = fmaf(dx, dx, dz * dz);
     const float c5 = dx * P.st - dz * P.ct;
-    const float c6 = log1pf(__fdividef(P.ds * fmaf(2.0f, c1, P.ds), c2));
+    const float x = __fdividef(P.ds * fmaf(2.0f, c1, P.ds), c2);
+    const float c6 = fabsf(x) < 0.5f ? log1pf(x)
+                                     : logf(__fdividef(fmaf(dxe, dxe, dze * dze), c2));
     const float c7 = atan2f(c5 * P.ds, fmaf(c1, P.ds, c2));
     const float c8 = dx * P.s2 + dz * P.c2;
     const float c9 = dx * P.c2 - dz * P.s2;
@@ -249,9 +255,12 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         double* sc2 = sst + np;
         double* ss2 = sc2 + np;
         double* sg = ss2 + np;
-        // FP32 layout after xc, zc: np PanelF32 records, then np gamma_j and
-        // np (gamma_{j+1} - gamma_j) (wrapping at the last panel)
-        PanelF32* fpan = reinterpret_cast<PanelF32*>(szc + np);
+        // FP32 layout after xc, zc: the panel ends (FP64), np PanelF32
+        // records, then np gamma_j and np (gamma_{j+1} - gamma_j) (wrapping at
+        // the last panel)
+        double* sex = szc + np;
+        double* sez = sex + np;
+        PanelF32* fpan = reinterpret_cast<PanelF32*>(sez + np);
         float* fg = reinterpret_cast<float*>(fpan + np);
         float* fdg = fg + np;
         if (s_loaded != k) {
@@ -260,6 +269,8 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
                 szc[j] = d.zc[j];
                 if (f32) {
                     const double dsj = d.ds[j];
+                    sex[j] = d.xc[j] + dsj * d.cth[j];
+                    sez[j] = d.zc[j] + dsj * d.sth[j];
                     fpan[j] = PanelF32{(float)d.cth[j], (float)d.sth[j], (float)dsj,
                                        (float)(1.0 / dsj), (float)d.c2th[j], (float)d.s2th[j]};
                     const double g0 = d.gamma[j], g1 = d.gamma[j == np - 1 ? 0 : j + 1];
@@ -285,7 +296,8 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
             if (f32) {
 #pragma unroll 2
                 for (int j = 0; j < np; ++j)
-                    sheet_pair_f32((float)(xi - sxc[j]), (float)(zi - szc[j]), fpan[j], fg[j],
+                    sheet_pair_f32((float)(xi - sxc[j]), (float)(zi - szc[j]),
+                                   (float)(xi - sex[j]), (float)(zi - sez[j]), fpan[j], fg[j],
                                    fdg[j], us, ws);
             } else {
                 for (int j = 0; j < np; ++j) {
