@@ -363,6 +363,23 @@ def run_ours(args, dist):
         s.push_uniforms(u)
     setup_s = time.perf_counter() - t_setup
 
+    # pair-kernel launch shape for this batch's class (result-invariant), and
+    # for the single-simulation classes the plain path uses
+    tune = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        b = ctx.autotune(sims, reps=1)
+        singles = set()
+        for s in sims:
+            c = ctx.shape_class([s])
+            if c not in singles:
+                singles.add(c)
+                ctx.autotune([s], reps=1)
+        tune = {"batch_class": b["shape_class"], "best": b["best"], "best_ms": b["best_ms"],
+                "default_ms": b["default_ms"], "candidates": len(b["candidates"]),
+                "single_sim_classes_tuned": len(singles),
+                "tuning_s": time.perf_counter() - t0}
+
     # warm-up (first step eager, then graph captured and replayed)
     ctx.step_batch(sims, args.warmup, use_graph=True)
     for s in sims:
@@ -498,6 +515,7 @@ def run_ours(args, dist):
                                     f"that file has no FP32 figure",
                      "share_of_step": nb_ms / max(prof["step"][0], 1e-9)},
         "profile_ms_per_step": {k: v[0] / max(args.prof_steps, 1) for k, v in prof.items()},
+        "autotune": tune,
         "gpu_launches": int(launches),
         "gpu_launches_note": "own kernels in the timed region; each step's Morton sort adds "
                              "the CUB radix-sort kernels compiled into the same library "
@@ -527,7 +545,7 @@ def run_ours(args, dist):
         from dvmpp_b200 import cases
 
         sv = cases.run_serving(args.serve_requests, 7, 20.0, (20, 100), (64, 512), 256, 100.0,
-                               True, True)
+                               True, True, autotune=not args.no_autotune)
         b, s = sv["batched"], sv["serial"]
         line["serving"] = {
             "requests": args.serve_requests, "arrivals": "Poisson 20 req/s (seed 7), realtime",
@@ -554,6 +572,8 @@ def main(argv=None):
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the built-in pair-kernel launch shape")
     ap.add_argument("--nbody-n", type=int, default=1 << 20,
                     help="standalone N-body leg size (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=40,

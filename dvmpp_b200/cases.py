@@ -93,7 +93,7 @@ def serve_params(r) -> N.Params:
 
 def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, max_active: int,
                 budget_gb: float, realtime: bool, serial_too: bool, graph: bool = True,
-                sync: bool = True):
+                sync: bool = True, autotune: bool = False):
     """The serving workload, continuous batching and (optionally) the plain
     serial path on the same requests; returns both summaries."""
     reqs = W.serving_requests(count, seed, rate, steps_range, panels_range)
@@ -106,6 +106,7 @@ def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, m
         srv = N.Server(ctx, budget_bytes=int(budget_gb * 2**30), max_active=max_active)
         srv.set_option(N.SERVE_GRAPH, 1 if graph else 0)
         srv.set_option(N.SERVE_SYNC, 1 if sync else 0)
+        srv.set_option(N.SERVE_AUTOTUNE, 1 if autotune else 0)
         for r in reqs:
             srv.submit(serve_params(r), *r["body"], r["steps"], r["arrival"])
         srv.run(serial=serial, realtime=realtime)
@@ -234,6 +235,8 @@ def main(argv=None):
     sv.add_argument("--serial", action="store_true", help="also run the plain serial path")
     sv.add_argument("--no-graph", action="store_true")
     sv.add_argument("--no-sync", action="store_true")
+    sv.add_argument("--autotune", action="store_true",
+                    help="tune the pair kernel once per new batch-shape class")
     pr = sub.add_parser("precision")
     pr.add_argument("--steps", type=int, default=20)
     pr.add_argument("--n-wake", type=int, default=1 << 19)
@@ -245,7 +248,7 @@ def main(argv=None):
     if a.cmd == "serve":
         print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
                                      a.max_active, a.budget_gb, a.realtime, a.serial,
-                                     not a.no_graph, not a.no_sync)))
+                                     not a.no_graph, not a.no_sync, a.autotune)))
     if a.cmd == "nbody":
         precs = {"f32": [N.F32], "f64": [N.F64], "both": [N.F32, N.F64]}[a.prec]
         print(json.dumps(run_nbody(a.n, precs, a.reps, a.seed)))

@@ -49,7 +49,8 @@ namespace {
 
 constexpr int kTableCap = 4096;
 constexpr size_t kMaxPlans = 32;       // cached batch plans per context (LRU)
-constexpr size_t kPoolPerPlan = 4096;  // list entries per plan: 4 partitions x 1024 sims
+constexpr size_t kPoolPerPlan = 6144;  // list entries per plan: 4 partitions + 1 reordered
+                                       // pair-kernel list, x 1024 sims
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -73,7 +74,38 @@ struct SubList {
     int n = 0;
     int max_np = 0;
     uint64_t total = 0;  // sum of capacities
+    std::vector<ListEntry> host;  // the entries as uploaded
+    // FP32 pair-kernel launch shape (from the context's tuning table) and, for
+    // order 1, the same entries costliest-first (the pair kernel's list only)
+    PairConfig cfg;
+    ListEntry* d_pair_list = nullptr;
 };
+
+// Batch-shape class of a tuning-table entry: log2 of the summed capacity of the
+// FP32 simulations (capacity, not the device-resident blob count, so a plan's
+// class is known on the host and stable) and a bucket of their number.
+int shape_class(uint64_t total_cap, int count) {
+    int lb = 0;
+    while (lb < 40 && (1ull << lb) < total_cap) ++lb;
+    const int cb = count <= 1 ? 0 : count <= 8 ? 1 : count <= 64 ? 2 : 3;
+    return lb * 4 + cb;
+}
+
+// Order 1: entries whose work items cost most (item cost ~ capacity / chunks
+// source pairs per target) first, ties in list order.
+std::vector<ListEntry> costliest_first(const std::vector<ListEntry>& h) {
+    std::vector<ListEntry> o(h);
+    std::stable_sort(o.begin(), o.end(), [](const ListEntry& a, const ListEntry& b) {
+        return (uint64_t)a.cap * (uint64_t)b.chunks > (uint64_t)b.cap * (uint64_t)a.chunks;
+    });
+    return o;
+}
+
+bool valid_pair_config(const dvm_pair_config& p) {
+    if (p.tile != 256 && p.tile != 128) return false;
+    if (p.ctas_per_sm < 1 || p.ctas_per_sm > (p.tile == 128 ? 4 : 3)) return false;
+    return p.order == 0 || p.order == 1;
+}
 
 struct Plan {
     std::vector<int> slots;            // the batch, in launch order
@@ -112,6 +144,11 @@ struct dvm_ctx {
     void* raw_block = nullptr;
     size_t raw_bytes = 0;
     std::map<std::vector<int>, Plan*> plans;
+    // pair-kernel launch shapes chosen by dvm_ctx_autotune / set by the caller
+    std::map<int, PairConfig> tuning;
+    bool tuning_default_set = false;
+    PairConfig tuning_default;
+    ListEntry* d_tune_list = nullptr;  // scratch list for the tuner (1024 entries)
     uint64_t plan_clock = 0;
     ListEntry* list_pool = nullptr;  // kMaxPlans slots of kPoolPerPlan entries
     std::vector<int> pool_free;
@@ -165,9 +202,17 @@ void drop_plans_with(dvm_ctx* c, int slot) {
     }
 }
 
-int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl) {
+PairConfig tuned_config(const dvm_ctx* c, int cls) {
+    auto it = c->tuning.find(cls);
+    if (it != c->tuning.end()) return it->second;
+    return c->tuning_default_set ? c->tuning_default : PairConfig();
+}
+
+int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl, bool f32_pairs = false) {
     sl.n = (int)sl.slots.size();
     if (sl.n == 0) return DVM_OK;
+    if (pl.pool_used + (size_t)sl.n * (f32_pairs ? 2 : 1) > kPoolPerPlan)
+        return fail(DVM_ERR_STATE, "plan list pool exhausted");
     std::vector<ListEntry> h(sl.n);
     uint64_t coff = 0, poff = 0, roff = 0, cofs = 0;
     for (int k = 0; k < sl.n; ++k) {
@@ -200,6 +245,18 @@ int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl) {
     pl.pool_used += sl.n;
     CK(cudaMemcpyAsync(sl.d_list, h.data(), sizeof(ListEntry) * sl.n, cudaMemcpyHostToDevice,
                        c->stream));
+    sl.host = h;
+    if (f32_pairs) {
+        sl.cfg = tuned_config(c, shape_class(sl.total, sl.n));
+        sl.d_pair_list = sl.d_list;
+        if (sl.cfg.order == 1 && sl.n > 1) {
+            const std::vector<ListEntry> o = costliest_first(h);
+            sl.d_pair_list = c->list_pool + (size_t)pl.pool_slot * kPoolPerPlan + pl.pool_used;
+            pl.pool_used += sl.n;
+            CK(cudaMemcpyAsync(sl.d_pair_list, o.data(), sizeof(ListEntry) * sl.n,
+                               cudaMemcpyHostToDevice, c->stream));
+        }
+    }
     return DVM_OK;
 }
 
@@ -338,7 +395,10 @@ void issue_step(dvm_ctx* c, Plan& pl) {
         biot_savart_prepare(T, S, sl.d_list, sl.n, prec, ws, sms, s);
         prof_end(c, p);
         p = prof_begin(c, DVM_PROF_NBODY);
-        biot_savart_compute(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        if (prec == kF32)
+            biot_savart_compute(T, S, sl.d_pair_list, sl.n, prec, ws, sms, s, sl.cfg);
+        else
+            biot_savart_compute(T, S, sl.d_list, sl.n, prec, ws, sms, s);
         prof_end(c, p);
         p = prof_begin(c, DVM_PROF_SORT);
         biot_savart_finish(T, S, sl.d_list, sl.n, prec, ws, sms, s);
@@ -441,7 +501,7 @@ int get_plan(dvm_ctx* c, const std::vector<int>& slots, Plan** out) {
     SubList* subs[] = {&pl->all, &pl->euler, &pl->rk3, &pl->rk3_f32, &pl->rk3_f64,
                        &pl->eul_f32, &pl->eul_f64, &pl->refl, &pl->del};
     for (SubList* s : subs) {
-        const int rc = build_sublist(c, *s, *pl);
+        const int rc = build_sublist(c, *s, *pl, s == &pl->rk3_f32 || s == &pl->eul_f32);
         if (rc) {
             free_plan(c, pl);
             return rc;
@@ -611,6 +671,7 @@ int dvm_ctx_destroy(dvm_ctx* c) {
     if (c->ws_block) cudaFree(c->ws_block);
     if (c->raw_block) cudaFree(c->raw_block);
     if (c->list_pool) cudaFree(c->list_pool);
+    if (c->d_tune_list) cudaFree(c->d_tune_list);
     if (c->d_table) cudaFree(c->d_table);
     if (c->d_state) cudaFree(c->d_state);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1154,7 +1215,8 @@ int dvm_sim_phase(dvm_sim* s, int phase) {
             biot_savart_prepare(T, S, L, 1, prec, ws, c->sms, st);
             prof_end(c, pr);
             pr = prof_begin(c, DVM_PROF_NBODY);
-            biot_savart_compute(T, S, L, 1, prec, ws, c->sms, st);
+            biot_savart_compute(T, S, L, 1, prec, ws, c->sms, st,
+                                tuned_config(c, shape_class(s->h.cap, 1)));
             prof_end(c, pr);
             pr = prof_begin(c, DVM_PROF_SORT);
             biot_savart_finish(T, S, L, 1, prec, ws, c->sms, st);
@@ -1168,7 +1230,8 @@ int dvm_sim_phase(dvm_sim* s, int phase) {
         case DVM_PHASE_SHEETBC: sheet_velocity(T, S, L, 1, 0, np, ws, c->sms, st); break;
         case DVM_PHASE_CONVECT:
             for (int k = 0; k < (s->h.scheme == kRK3 ? 3 : 1); ++k) {
-                biot_savart_self(T, S, L, 1, prec, ws, c->sms, st);
+                biot_savart_self(T, S, L, 1, prec, ws, c->sms, st,
+                                 tuned_config(c, shape_class(s->h.cap, 1)));
                 sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
                 sheet_solve(T, S, L, 1, np, st);
                 sheet_velocity(T, S, L, 1, s->h.scheme == kRK3 ? 2 + k : 1, np, ws, c->sms, st);
@@ -1210,6 +1273,157 @@ int dvm_step_batch(dvm_ctx* c, dvm_sim* const* sims, int nsims, int nsteps, int 
         slots[i] = sims[i]->slot;
     }
     return run_steps(c, slots, nsteps, use_graph != 0);
+}
+
+// ---- pair-kernel autotuning ------------------------------------------------------------
+namespace {
+const dvm_pair_config kCandidates[] = {
+    {256, 3, 0, 0}, {256, 2, 0, 0}, {256, 1, 0, 0}, {256, 3, 1, 0}, {256, 2, 1, 0},
+    {256, 1, 1, 0}, {128, 4, 0, 0}, {128, 3, 0, 0}, {128, 2, 0, 0}, {128, 1, 0, 0},
+    {128, 4, 1, 0}, {128, 3, 1, 0}, {128, 2, 1, 0}, {128, 1, 1, 0}};
+constexpr int kNumCandidates = (int)(sizeof(kCandidates) / sizeof(kCandidates[0]));
+static_assert(kNumCandidates <= DVM_TUNE_MAX_CANDIDATES, "candidate table too long");
+
+PairConfig to_internal(const dvm_pair_config& p) {
+    PairConfig c;
+    c.tile = p.tile;
+    c.ctas = p.ctas_per_sm;
+    c.order = p.order;
+    return c;
+}
+dvm_pair_config to_abi(const PairConfig& c) { return dvm_pair_config{c.tile, c.ctas, c.order, 0}; }
+
+int f32_members(dvm_ctx* c, dvm_sim* const* sims, int nsims, std::vector<int>& slots,
+                uint64_t& total_cap) {
+    slots.clear();
+    total_cap = 0;
+    for (int i = 0; i < nsims; ++i) {
+        if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        if (sims[i]->h.precision != kF32) continue;
+        if (std::find(slots.begin(), slots.end(), sims[i]->slot) != slots.end())
+            return fail(DVM_ERR_ARG, "simulation listed twice");
+        slots.push_back(sims[i]->slot);
+        total_cap += sims[i]->h.cap;
+    }
+    return DVM_OK;
+}
+}  // namespace
+
+int dvm_tune_candidate(int index, dvm_pair_config* out) {
+    if (!out || index < 0 || index >= kNumCandidates) return fail(DVM_ERR_ARG, "no such candidate");
+    *out = kCandidates[index];
+    return DVM_OK;
+}
+
+int dvm_batch_shape_class(dvm_ctx* c, dvm_sim* const* sims, int nsims, int* cls) {
+    if (!c || !cls || nsims < 0 || (nsims && !sims)) return fail(DVM_ERR_ARG, "bad argument");
+    std::vector<int> slots;
+    uint64_t total = 0;
+    const int rc = f32_members(c, sims, nsims, slots, total);
+    if (rc) return rc;
+    *cls = slots.empty() ? -1 : shape_class(total, (int)slots.size());
+    return DVM_OK;
+}
+
+int dvm_ctx_set_pair_config(dvm_ctx* c, int cls, const dvm_pair_config* cfg) {
+    if (!c || !cfg || cls < -1) return fail(DVM_ERR_ARG, "bad argument");
+    if (!valid_pair_config(*cfg)) return fail(DVM_ERR_ARG, "invalid pair-kernel configuration");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));  // graphs of the old shapes are about to go
+    if (cls == -1) {
+        c->tuning.clear();
+        c->tuning_default = to_internal(*cfg);
+        c->tuning_default_set = true;
+    } else {
+        c->tuning[cls] = to_internal(*cfg);
+    }
+    drop_plans_with(c, -1);
+    return DVM_OK;
+}
+
+int dvm_ctx_get_pair_config(dvm_ctx* c, int cls, dvm_pair_config* out) {
+    if (!c || !out) return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    *out = to_abi(tuned_config(c, cls));
+    return DVM_OK;
+}
+
+int dvm_ctx_autotune(dvm_ctx* c, dvm_sim* const* sims, int nsims, int reps, dvm_tune_result* out) {
+    if (!c || !out || nsims <= 0 || nsims > 1024 || !sims) return fail(DVM_ERR_ARG, "bad argument");
+    reps = std::max(1, std::min(reps, 100));
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    std::vector<int> slots;
+    uint64_t total = 0;
+    int rc = f32_members(c, sims, nsims, slots, total);
+    if (rc) return rc;
+    if (slots.empty()) return fail(DVM_ERR_ARG, "no FP32 simulation in the batch");
+    std::sort(slots.begin(), slots.end());
+    Plan* pl = nullptr;
+    rc = get_plan(c, slots, &pl);  // its `all` list is exactly the FP32 members
+    if (rc) return rc;
+    rc = ensure_workspace(c, pl->ws_need_cap, pl->part_elems, pl->rhs_elems, pl->circ_elems,
+                          (int)slots.size(), pl->need_delete);
+    if (rc) return rc;
+    if (!c->d_tune_list) CK(cudaMalloc(&c->d_tune_list, sizeof(ListEntry) * 1024));
+    const SubList& sl = pl->all;
+    const std::vector<ListEntry> ordered = costliest_first(sl.host);
+    CK(cudaMemcpyAsync(c->d_tune_list, ordered.data(), sizeof(ListEntry) * sl.n,
+                       cudaMemcpyHostToDevice, c->stream));
+    Workspace ws = c->ws;
+    ws.total_cap = sl.total;
+    ws.key_bits = key_bits_for(sl.n);
+    InstDesc* T = c->d_table;
+    InstState* S = c->d_state;
+    biot_savart_prepare(T, S, sl.d_list, sl.n, kF32, ws, c->sms, c->stream);
+    cudaEvent_t a = nullptr, b = nullptr;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    auto launch = [&](const dvm_pair_config& p) {
+        cudaMemsetAsync(ws.work, 0, sizeof(unsigned), c->stream);
+        biot_savart_compute(T, S, p.order == 1 ? c->d_tune_list : sl.d_list, sl.n, kF32, ws,
+                            c->sms, c->stream, to_internal(p));
+    };
+    int err = DVM_OK;
+    // one untimed launch of each kernel variant (module load, caches)
+    launch(kCandidates[0]);
+    launch(kCandidates[6]);
+    std::memset(out, 0, sizeof(*out));
+    out->shape_class = shape_class(total, (int)slots.size());
+    out->candidates = kNumCandidates;
+    int best = 0;
+    for (int k = 0; k < kNumCandidates && !err; ++k) {
+        double ms = 0.0;
+        for (int r = 0; r < reps; ++r) {
+            cudaMemsetAsync(ws.work, 0, sizeof(unsigned), c->stream);
+            cudaEventRecord(a, c->stream);
+            biot_savart_compute(T, S, kCandidates[k].order == 1 ? c->d_tune_list : sl.d_list,
+                                sl.n, kF32, ws, c->sms, c->stream, to_internal(kCandidates[k]));
+            cudaEventRecord(b, c->stream);
+            float t = 0.f;
+            if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&t, a, b) != cudaSuccess) {
+                err = fail(DVM_ERR_CUDA, std::string("autotune: ") +
+                                             cudaGetErrorString(cudaGetLastError()));
+                break;
+            }
+            ms += t;
+        }
+        out->ms[k] = ms / reps;
+        if (out->ms[k] < out->ms[best]) best = k;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (err) return err;
+    CK(cudaGetLastError());
+    g_launches += 4 + (uint64_t)kNumCandidates * reps;  // keys + pack, 2 warm-ups, the timed ones
+    out->best = kCandidates[best];
+    out->best_ms = out->ms[best];
+    out->default_ms = out->ms[0];
+    c->tuning[out->shape_class] = to_internal(out->best);
+    CK(cudaStreamSynchronize(c->stream));
+    drop_plans_with(c, -1);  // plans and graphs rebuild with the tuned shape
+    return DVM_OK;
 }
 
 // ---- plugin seam ---------------------------------------------------------------------
@@ -1270,7 +1484,8 @@ static int raw_self(dvm_ctx* c, const double* x, const double* z, const double* 
     Workspace ws = c->ws;
     ws.key_bits = key_bits_for(1);
     ws.total_cap = cap;
-    biot_savart_self(c->d_table, c->d_state, d_list, 1, precision, ws, c->sms, c->stream);
+    biot_savart_self(c->d_table, c->d_state, d_list, 1, precision, ws, c->sms, c->stream,
+                     tuned_config(c, shape_class(cap, 1)));
     g_launches += precision == kF32 ? 4 : 3;
     CK(cudaGetLastError());
     return DVM_OK;

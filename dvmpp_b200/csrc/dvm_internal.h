@@ -155,16 +155,27 @@ int report_error(int code, const char* msg);
 // ---- launchers (all asynchronous on `s`) ------------------------------------
 size_t cub_sort_bytes(uint64_t total);
 
+// Launch shape of the FP32 pair kernel.  None of it changes a result: the
+// source chunking (which does) is fixed by each simulation's capacity.
+struct PairConfig {
+    int tile = 256;  // targets per work item: 256 or 128
+    int ctas = 3;    // persistent CTAs per SM
+    int order = 0;   // 0: list order; 1: costliest simulations' items first (the caller
+                     // passes the list in that order)
+};
+
 // Self-induced Biot-Savart (src/VelocityKernel.cpp:30-67) for every listed sim:
 // FP32 + compensated sums over spatially sorted blobs, or FP64 in blob order.
 void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-                      int precision, const Workspace& ws, int sms, cudaStream_t s);
+                      int precision, const Workspace& ws, int sms, cudaStream_t s,
+                      const PairConfig& cfg = PairConfig());
 // The same in three parts (sort + pack / pair kernel / combine + scatter), so
 // the pair kernel can be timed on its own.
 void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                          int precision, const Workspace& ws, int sms, cudaStream_t s);
 void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-                         int precision, const Workspace& ws, int sms, cudaStream_t s);
+                         int precision, const Workspace& ws, int sms, cudaStream_t s,
+                         const PairConfig& cfg = PairConfig());
 void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                         int precision, const Workspace& ws, int sms, cudaStream_t s);
 // Blob-on-collocation right-hand side b (src/VortexSheet.cpp:171-210).

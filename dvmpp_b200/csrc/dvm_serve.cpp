@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -56,6 +57,9 @@ struct dvm_server {
     bool ran = false;
     bool graph = true;       // DVM_SERVE_GRAPH
     bool sync_tick = true;   // DVM_SERVE_SYNC
+    bool autotune = false;   // DVM_SERVE_AUTOTUNE
+    std::set<int> tuned;     // shape classes already tuned
+    uint32_t tunings = 0;
 };
 
 extern "C" {
@@ -91,6 +95,7 @@ int dvm_server_set_option(dvm_server* s, int option, int value) {
     switch (option) {
         case DVM_SERVE_GRAPH: s->graph = value != 0; return DVM_OK;
         case DVM_SERVE_SYNC: s->sync_tick = value != 0; return DVM_OK;
+        case DVM_SERVE_AUTOTUNE: s->autotune = value != 0; return DVM_OK;
         default: return dvmk::report_error(DVM_ERR_ARG, "dvm_server_set_option: unknown option");
     }
 }
@@ -191,6 +196,17 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
         // With DVM_SERVE_SYNC each tick is waited for (device status read per
         // simulation); without it the host runs ahead and the status of a
         // simulation is read only when it retires (step counts are host-known).
+        if (s->autotune) {  // once per new shape class (tuning never changes results)
+            int cls = -1;
+            int rc = dvm_batch_shape_class(s->ctx, batch.data(), (int)batch.size(), &cls);
+            if (rc) return rc;
+            if (cls >= 0 && s->tuned.insert(cls).second) {
+                dvm_tune_result tr;
+                rc = dvm_ctx_autotune(s->ctx, batch.data(), (int)batch.size(), 1, &tr);
+                if (rc) return rc;
+                ++s->tunings;
+            }
+        }
         int rc = dvm_step_batch(s->ctx, batch.data(), (int)batch.size(), 1, s->graph ? 1 : 0);
         if (rc) return rc;
         ++ticks;

@@ -183,9 +183,10 @@ __device__ __forceinline__ uint32_t chunk_size(uint32_t n, int chunks) {
 // against one source chunk.  The warp stages its own source tiles in shared
 // memory and never waits for other warps, so far-path and near-path warps of a
 // block do not hold each other up at barriers.
-constexpr int kWR = 8;                // consecutive targets per lane
-constexpr int kWP = kWR / 2;          // target pairs per lane (packed FP32x2)
-constexpr int kWTT = 32 * kWR;        // targets per warp item
+// Work-item shape: WR consecutive sorted targets per lane (WR / 2 packed
+// FP32x2 target pairs), 32 * WR targets per warp item.  WR is 8 (256-target
+// items) or 4 (128-target items); the choice changes which targets share a
+// warp, never a target's own operation sequence, so results do not depend on it.
 constexpr int kWWarps = 4;            // independent warps per block
 #ifndef DVM_SELF_MINBLOCKS
 #define DVM_SELF_MINBLOCKS 3          // blocks per SM the register budget is sized for
@@ -232,7 +233,7 @@ struct StagedSrc {
     float4 b;
 };
 
-// Target pairs (of kWP per lane) whose two reciprocals share one MUFU.RCP.
+// Target pairs (of WR / 2 per lane) whose two reciprocals share one MUFU.RCP.
 #ifndef DVM_PAIR_RCP
 #define DVM_PAIR_RCP 0
 #endif
@@ -243,16 +244,17 @@ constexpr int kPairRcp = DVM_PAIR_RCP;
 constexpr int kFarUnroll = DVM_FAR_UNROLL;  // sources per unrolled far-loop body
 
 // Far pairs: no core test.  Accumulates -u (so every update is one FMA) and w.
+template <int WP>
 __device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
-                                          const uint64_t (&tx2)[kWP], const uint64_t (&tz2)[kWP],
-                                          uint64_t (&nu2)[kWP], uint64_t (&w2)[kWP]) {
+                                          const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
+                                          uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
 #pragma unroll kFarUnroll
     for (int jj = 0; jj < kBsST; ++jj) {
         const float4 A = src[jj].a;
         const float4 B = src[jj].b;
         const uint64_t sx = f2pack(A.x, A.y), sz = f2pack(A.z, A.w), sg = f2pack(B.x, B.y);
 #pragma unroll
-        for (int q = 0; q < kWP; ++q) {
+        for (int q = 0; q < WP; ++q) {
             const uint64_t dx = f2sub(tx2[q], sx);
             const uint64_t dz = f2sub(tz2[q], sz);
             const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
@@ -286,12 +288,14 @@ __device__ __forceinline__ float core_kernel(float r2, float rs, float rcp_r2) {
 }
 
 // Near pairs: the reference's exact test per pair (scalar; rare).
+template <int WP>
 __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
-                                           const uint64_t (&tx2)[kWP], const uint64_t (&tz2)[kWP],
-                                           uint64_t (&nu2)[kWP], uint64_t (&w2)[kWP]) {
-    float nu[kWR], w[kWR], tx[kWR], tz[kWR];
+                                           const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
+                                           uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
+    constexpr int WR = 2 * WP;
+    float nu[WR], w[WR], tx[WR], tz[WR];
 #pragma unroll
-    for (int q = 0; q < kWP; ++q) {
+    for (int q = 0; q < WP; ++q) {
         tx[2 * q] = f2lo(tx2[q]);
         tx[2 * q + 1] = f2hi(tx2[q]);
         tz[2 * q] = f2lo(tz2[q]);
@@ -306,7 +310,7 @@ __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
         const float4 A = src[jj].a;
         const float4 B = src[jj].b;
 #pragma unroll
-        for (int r = 0; r < kWR; ++r) {
+        for (int r = 0; r < WR; ++r) {
             const float dx = tx[r] - A.x;
             const float dz = tz[r] - A.z;
             const float r2 = fmaf(dx, dx, dz * dz);
@@ -318,7 +322,7 @@ __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
         }
     }
 #pragma unroll
-    for (int q = 0; q < kWP; ++q) {
+    for (int q = 0; q < WP; ++q) {
         nu2[q] = f2pack(nu[2 * q], nu[2 * q + 1]);
         w2[q] = f2pack(w[2 * q], w[2 * q + 1]);
     }
@@ -331,7 +335,8 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     s = t;
 }
 
-__global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
+template <int WR, int MINB>
+__global__ void __launch_bounds__(32 * kWWarps, MINB)
     k_self_f32(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
                const double2* __restrict__ pxz, const float4* __restrict__ pf,
                const TileMeta* __restrict__ meta, double2* __restrict__ part,
@@ -339,6 +344,7 @@ __global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ StagedSrc s_src[kWWarps][kBsST];
     __shared__ double s_box[kWWarps][4];
+    constexpr int kWP = WR / 2, kWTT = 32 * WR;
     if (threadIdx.x == 0) {
         unsigned acc = 0;
         for (int k = 0; k < nlist; ++k) {
@@ -370,7 +376,7 @@ __global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
 
         uint64_t tx2[kWP], tz2[kWP];
         double wxmin = DBL_MAX, wxmax = -DBL_MAX, wzmin = DBL_MAX, wzmax = -DBL_MAX;
-        const uint32_t tb = t0 + lane * kWR;
+        const uint32_t tb = t0 + lane * WR;
 #pragma unroll
         for (int q = 0; q < kWP; ++q) {
             float xs[2], zs[2];
@@ -406,9 +412,9 @@ __global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
             s_box[wid][2] = wzmin;
             s_box[wid][3] = wzmax;
         }
-        float su[kWR], cu[kWR], sw[kWR], cw[kWR];  // Kahan sums of -u and w
+        float su[WR], cu[WR], sw[WR], cw[WR];  // Kahan sums of -u and w
 #pragma unroll
-        for (int r = 0; r < kWR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
+        for (int r = 0; r < WR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
 
         for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
             __syncwarp();
@@ -450,7 +456,7 @@ __global__ void __launch_bounds__(32 * kWWarps, DVM_SELF_MINBLOCKS)
         }
         double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
 #pragma unroll
-        for (int r = 0; r < kWR; ++r)
+        for (int r = 0; r < WR; ++r)
             if (tb + r < n)
                 out[tb + r] = make_double2(-((double)su[r] - (double)cu[r]),
                                            (double)sw[r] - (double)cw[r]);
@@ -770,15 +776,22 @@ void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* 
 }
 
 void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-                         int precision, const Workspace& ws, int sms, cudaStream_t s) {
+                         int precision, const Workspace& ws, int sms, cudaStream_t s,
+                         const PairConfig& cfg) {
     (void)table;
-    if (precision == kF32)
-        k_self_f32<<<sms * DVM_SELF_MINBLOCKS, 32 * kWWarps, 0, s>>>(
-            st, list, nlist, reinterpret_cast<const double2*>(ws.packed),
-            reinterpret_cast<const float4*>(ws.packed + ws.packed_cap / 2), ws.meta, ws.part,
-            ws.work);
-    else
+    if (precision == kF32) {
+        const double2* pxz = reinterpret_cast<const double2*>(ws.packed);
+        const float4* pf = reinterpret_cast<const float4*>(ws.packed + ws.packed_cap / 2);
+        const int g = sms * std::max(1, std::min(cfg.ctas, 4));
+        if (cfg.tile == 128)
+            k_self_f32<4, 4><<<g, 32 * kWWarps, 0, s>>>(st, list, nlist, pxz, pf, ws.meta,
+                                                         ws.part, ws.work);
+        else
+            k_self_f32<8, DVM_SELF_MINBLOCKS><<<g, 32 * kWWarps, 0, s>>>(
+                st, list, nlist, pxz, pf, ws.meta, ws.part, ws.work);
+    } else {
         k_self_f64<<<sms, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part, ws.work);
+    }
 }
 
 void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
@@ -788,9 +801,10 @@ void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* l
 }
 
 void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-                      int precision, const Workspace& ws, int sms, cudaStream_t s) {
+                      int precision, const Workspace& ws, int sms, cudaStream_t s,
+                      const PairConfig& cfg) {
     biot_savart_prepare(table, st, list, nlist, precision, ws, sms, s);
-    biot_savart_compute(table, st, list, nlist, precision, ws, sms, s);
+    biot_savart_compute(table, st, list, nlist, precision, ws, sms, s, cfg);
     biot_savart_finish(table, st, list, nlist, precision, ws, sms, s);
 }
 

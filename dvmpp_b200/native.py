@@ -230,6 +230,37 @@ class Context:
         arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
         _check(self.lib.dvm_step_batch(self.h, arr, len(sims), nsteps, 1 if use_graph else 0))
 
+    # ---- pair-kernel autotuning
+    @staticmethod
+    def _sim_array(sims):
+        return (C.c_void_p * len(sims))(*[s.h for s in sims])
+
+    def autotune(self, sims, reps: int = 1) -> dict:
+        """Time every pair-kernel launch shape on this batch and keep the best
+        for its shape class; returns the candidates' times."""
+        r = TuneResult()
+        _check(self.lib.dvm_ctx_autotune(self.h, self._sim_array(sims), len(sims), reps,
+                                         C.byref(r)))
+        cands = tune_candidates()
+        return {"shape_class": r.shape_class, "best": r.best.as_dict(), "best_ms": r.best_ms,
+                "default_ms": r.default_ms,
+                "candidates": [dict(c, ms=r.ms[k]) for k, c in enumerate(cands[:r.candidates])]}
+
+    def shape_class(self, sims) -> int:
+        v = C.c_int()
+        _check(self.lib.dvm_batch_shape_class(self.h, self._sim_array(sims), len(sims),
+                                              C.byref(v)))
+        return v.value
+
+    def set_pair_config(self, shape_class: int, tile: int, ctas_per_sm: int, order: int):
+        cfg = PairConfig(tile, ctas_per_sm, order, 0)
+        _check(self.lib.dvm_ctx_set_pair_config(self.h, shape_class, C.byref(cfg)))
+
+    def pair_config(self, shape_class: int) -> dict:
+        cfg = PairConfig()
+        _check(self.lib.dvm_ctx_get_pair_config(self.h, shape_class, C.byref(cfg)))
+        return cfg.as_dict()
+
     def sim(self, params: "Params", xp, zp) -> "Simulation":
         return Simulation(self, params, xp, zp)
 
@@ -378,7 +409,7 @@ class Simulation:
 
 
 # ---- serving ----------------------------------------------------------------
-SERVE_GRAPH, SERVE_SYNC = 0, 1
+SERVE_GRAPH, SERVE_SYNC, SERVE_AUTOTUNE = 0, 1, 2
 
 
 class RequestResult(C.Structure):
@@ -396,6 +427,43 @@ class ServerSummary(C.Structure):
                 ("latency_mean_s", C.c_double), ("queue_p50_s", C.c_double),
                 ("queue_p99_s", C.c_double), ("peak_active", C.c_uint32),
                 ("peak_bytes", C.c_uint64)]
+
+
+class PairConfig(C.Structure):
+    _fields_ = [("tile", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32),
+                ("reserved", C.c_int32)]
+
+    def as_dict(self):
+        return {"tile": self.tile, "ctas_per_sm": self.ctas_per_sm, "order": self.order}
+
+
+TUNE_MAX_CANDIDATES = 16
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("best", PairConfig), ("shape_class", C.c_int32), ("candidates", C.c_int32),
+                ("best_ms", C.c_double), ("default_ms", C.c_double),
+                ("ms", C.c_double * TUNE_MAX_CANDIDATES)]
+
+
+def tune_candidates() -> list:
+    """The autotuner's search space, in the order it times it."""
+    lib = load()
+    out, k = [], 0
+    cfg = PairConfig()
+    while lib.dvm_tune_candidate(k, C.byref(cfg)) == OK:
+        out.append(cfg.as_dict())
+        k += 1
+    return out
+
+
+SIGNATURES.update({
+    "dvm_tune_candidate": (C.c_int, [C.c_int, C.POINTER(PairConfig)]),
+    "dvm_ctx_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(TuneResult)]),
+    "dvm_batch_shape_class": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "dvm_ctx_set_pair_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PairConfig)]),
+    "dvm_ctx_get_pair_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PairConfig)]),
+})
 
 
 SIGNATURES.update({

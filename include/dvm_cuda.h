@@ -29,6 +29,8 @@
  *                                                               src/DVMBase.cpp:86-133,145-149
  *   dvm_sim_push_uniforms     Random::rand stream feed          src/Random.cpp:8-18
  *   dvm_step_batch            (no counterpart: many simulations per launch)
+ *   dvm_ctx_autotune          (no counterpart: pair-kernel launch shapes)
+ *   dvm_server_*              (no counterpart: continuous-batching request loop)
  */
 #ifndef DVM_CUDA_H
 #define DVM_CUDA_H
@@ -56,7 +58,8 @@ extern "C" {
 
 /* arithmetic of the pair interactions */
 #define DVM_F64 0 /* FP64, reference operation order */
-#define DVM_F32 1 /* FP32 with compensated sums (sheet-on-blob stays FP64) */
+#define DVM_F32 1 /* FP32 pair terms with compensated / FP64 sums; FP64 state, QR,
+                     refinement residual and Kelvin row */
 
 #define DVM_EULER 0 /* Scheme::Euler, src/DVMBase.hpp:27-30 */
 #define DVM_RK3 1   /* Scheme::RK3 */
@@ -245,6 +248,46 @@ int dvm_sim_step(dvm_sim* sim, int nsteps);
  * (re-used while the list is unchanged).  Asynchronous: check dvm_sim_status. */
 int dvm_step_batch(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int nsteps, int use_graph);
 
+/* ---- pair-kernel autotuning (no counterpart in the reference) ---------------------
+ * The FP32 blob-on-blob kernel's launch shape: targets per work item, persistent
+ * CTAs per SM and the order in which simulations' work items are handed out.
+ * None of these changes a result (source chunking, which would, is fixed by each
+ * simulation's capacity), so tuning never changes velocities.  Shapes are kept
+ * per batch-shape class (log2 of the summed capacity of the batch's FP32
+ * simulations x a bucket of their count: 1, 2-8, 9-64, more); plans and graphs
+ * built afterwards use them. */
+typedef struct dvm_pair_config {
+    int32_t tile;        /* targets per work item: 256 or 128 */
+    int32_t ctas_per_sm; /* 1..3 for 256-target items, 1..4 for 128 */
+    int32_t order;       /* 0: list order; 1: costliest simulations' items first */
+    int32_t reserved;
+} dvm_pair_config;
+
+#define DVM_TUNE_MAX_CANDIDATES 16
+typedef struct dvm_tune_result {
+    dvm_pair_config best;
+    int32_t shape_class;
+    int32_t candidates;          /* configurations timed (dvm_tune_candidate order) */
+    double best_ms;              /* mean pair-kernel time of the best */
+    double default_ms;           /* mean time of the built-in shape (256, 3, 0) */
+    double ms[DVM_TUNE_MAX_CANDIDATES];
+} dvm_tune_result;
+
+/* The search space, enumerated: index 0 .. count-1; DVM_ERR_ARG past the end. */
+int dvm_tune_candidate(int index, dvm_pair_config* out);
+/* Time every candidate on this batch's FP32 simulations (reps launches each,
+ * after one untimed launch per kernel variant) and store the fastest for the
+ * batch's class.  Simulation state is not modified (the pair kernel writes only
+ * workspace partials; the next step recomputes velocities). */
+int dvm_ctx_autotune(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int reps,
+                     dvm_tune_result* out);
+/* Class of a batch (-1: no FP32 simulation in it). */
+int dvm_batch_shape_class(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int* shape_class);
+/* Set / read the shape for one class; shape_class -1 sets the default for every
+ * class and clears the table.  Setting drops cached plans and graphs. */
+int dvm_ctx_set_pair_config(dvm_ctx* ctx, int shape_class, const dvm_pair_config* cfg);
+int dvm_ctx_get_pair_config(dvm_ctx* ctx, int shape_class, dvm_pair_config* out);
+
 /* ---- serving (no counterpart in the reference) ----------------------------------------
  * A request loop over one context: requests (a body, parameters and a step
  * count) arrive at given times; each is admitted as soon as it has arrived,
@@ -283,9 +326,12 @@ int dvm_server_destroy(dvm_server* srv);
 /* Options (before dvm_server_run): DVM_SERVE_GRAPH 1 captures the step in a CUDA
  * graph, re-used while the batch is unchanged (default 1); DVM_SERVE_SYNC 1
  * waits for each tick before the next admission (default 1; 0 lets the host
- * run ahead and reads device status only at retirement). */
+ * run ahead and reads device status only at retirement); DVM_SERVE_AUTOTUNE 1
+ * runs dvm_ctx_autotune (one launch per candidate) the first time a batch of a
+ * new shape class is stepped (default 0). */
 #define DVM_SERVE_GRAPH 0
 #define DVM_SERVE_SYNC 1
+#define DVM_SERVE_AUTOTUNE 2
 int dvm_server_set_option(dvm_server* srv, int option, int value);
 int dvm_server_submit(dvm_server* srv, const dvm_sim_params* p, const double* body_x,
                       const double* body_z, int npoints, uint32_t steps, double arrival_s,
