@@ -545,7 +545,7 @@ def run_ours(args, dist):
         from dvmpp_b200 import cases
 
         sv = cases.run_serving(args.serve_requests, 7, 20.0, (20, 100), (64, 512), 256, 100.0,
-                               True, True, autotune=not args.no_autotune)
+                               True, True)
         b, s = sv["batched"], sv["serial"]
         line["serving"] = {
             "requests": args.serve_requests, "arrivals": "Poisson 20 req/s (seed 7), realtime",

@@ -78,6 +78,7 @@ struct SubList {
     // FP32 pair-kernel launch shape (from the context's tuning table) and, for
     // order 1, the same entries costliest-first (the pair kernel's list only)
     PairConfig cfg;
+    int cls = -1;
     ListEntry* d_pair_list = nullptr;
 };
 
@@ -191,6 +192,18 @@ void free_plan(dvm_ctx* c, Plan* pl) {
     delete pl;
 }
 
+// Drop the plans (and graphs) whose FP32 pair lists belong to shape class cls.
+void drop_plans_of_class(dvm_ctx* c, int cls) {
+    for (auto it = c->plans.begin(); it != c->plans.end();) {
+        if (it->second->eul_f32.cls == cls || it->second->rk3_f32.cls == cls) {
+            free_plan(c, it->second);
+            it = c->plans.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
 void drop_plans_with(dvm_ctx* c, int slot) {
     for (auto it = c->plans.begin(); it != c->plans.end();) {
         if (slot < 0 || std::find(it->first.begin(), it->first.end(), slot) != it->first.end()) {
@@ -247,7 +260,8 @@ int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl, bool f32_pairs = false) {
                        c->stream));
     sl.host = h;
     if (f32_pairs) {
-        sl.cfg = tuned_config(c, shape_class(sl.total, sl.n));
+        sl.cls = shape_class(sl.total, sl.n);
+        sl.cfg = tuned_config(c, sl.cls);
         sl.d_pair_list = sl.d_list;
         if (sl.cfg.order == 1 && sl.n > 1) {
             const std::vector<ListEntry> o = costliest_first(h);
@@ -1335,10 +1349,28 @@ int dvm_ctx_set_pair_config(dvm_ctx* c, int cls, const dvm_pair_config* cfg) {
         c->tuning.clear();
         c->tuning_default = to_internal(*cfg);
         c->tuning_default_set = true;
+        drop_plans_with(c, -1);
     } else {
         c->tuning[cls] = to_internal(*cfg);
+        drop_plans_of_class(c, cls);
     }
-    drop_plans_with(c, -1);
+    return DVM_OK;
+}
+
+int dvm_ctx_tuning_table(dvm_ctx* c, int max_entries, int* classes, dvm_pair_config* cfgs,
+                         int* count) {
+    if (!c || !count || max_entries < 0 || (max_entries && (!classes || !cfgs)))
+        return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    int k = 0;
+    for (const auto& kv : c->tuning) {
+        if (k < max_entries) {
+            classes[k] = kv.first;
+            cfgs[k] = to_abi(kv.second);
+        }
+        ++k;
+    }
+    *count = k;
     return DVM_OK;
 }
 
@@ -1422,7 +1454,7 @@ int dvm_ctx_autotune(dvm_ctx* c, dvm_sim* const* sims, int nsims, int reps, dvm_
     out->default_ms = out->ms[0];
     c->tuning[out->shape_class] = to_internal(out->best);
     CK(cudaStreamSynchronize(c->stream));
-    drop_plans_with(c, -1);  // plans and graphs rebuild with the tuned shape
+    drop_plans_of_class(c, out->shape_class);  // they rebuild with the tuned shape
     return DVM_OK;
 }
 

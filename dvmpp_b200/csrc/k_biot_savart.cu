@@ -372,7 +372,10 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
         const uint32_t j0 = c * cs, j1 = min(n, j0 + cs);
         const double2* __restrict__ X = pxz + e.coff;
         const float4* __restrict__ F = pf + e.coff;
-        const double2 o = X[t0];  // the item's origin: its first target
+        // FP32 offsets are taken from the first target of the enclosing
+        // 256-target block, whatever the item size, so every item shape rounds
+        // a pair's offsets identically
+        const double2 o = X[t0 - t0 % 256u];
 
         uint64_t tx2[kWP], tz2[kWP];
         double wxmin = DBL_MAX, wxmax = -DBL_MAX, wzmin = DBL_MAX, wzmax = -DBL_MAX;

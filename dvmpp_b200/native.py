@@ -7,6 +7,7 @@ CUDA library is missing, or no B200 is visible, every call raises.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 from dataclasses import dataclass
 
@@ -261,6 +262,24 @@ class Context:
         _check(self.lib.dvm_ctx_get_pair_config(self.h, shape_class, C.byref(cfg)))
         return cfg.as_dict()
 
+    def tuning_table(self) -> dict:
+        """{shape_class: config} of every tuned class."""
+        n = C.c_int()
+        _check(self.lib.dvm_ctx_tuning_table(self.h, 0, None, None, C.byref(n)))
+        cls = (C.c_int * max(n.value, 1))()
+        cfgs = (PairConfig * max(n.value, 1))()
+        _check(self.lib.dvm_ctx_tuning_table(self.h, n.value, cls, cfgs, C.byref(n)))
+        return {int(cls[k]): cfgs[k].as_dict() for k in range(n.value)}
+
+    def save_tuning(self, path: str):
+        with open(path, "w") as f:
+            json.dump({str(k): v for k, v in self.tuning_table().items()}, f, indent=1)
+
+    def load_tuning(self, path: str):
+        with open(path) as f:
+            for k, v in json.load(f).items():
+                self.set_pair_config(int(k), v["tile"], v["ctas_per_sm"], v["order"])
+
     def sim(self, params: "Params", xp, zp) -> "Simulation":
         return Simulation(self, params, xp, zp)
 
@@ -463,6 +482,8 @@ SIGNATURES.update({
     "dvm_batch_shape_class": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "dvm_ctx_set_pair_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PairConfig)]),
     "dvm_ctx_get_pair_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PairConfig)]),
+    "dvm_ctx_tuning_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(PairConfig), C.POINTER(C.c_int)]),
 })
 
 

@@ -278,7 +278,8 @@ int dvm_tune_candidate(int index, dvm_pair_config* out);
 /* Time every candidate on this batch's FP32 simulations (reps launches each,
  * after one untimed launch per kernel variant) and store the fastest for the
  * batch's class.  Simulation state is not modified (the pair kernel writes only
- * workspace partials; the next step recomputes velocities). */
+ * workspace partials; the next step recomputes velocities).  Synchronous: meant
+ * for set-up (or once per class in a long-running server), not per step. */
 int dvm_ctx_autotune(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int reps,
                      dvm_tune_result* out);
 /* Class of a batch (-1: no FP32 simulation in it). */
@@ -287,6 +288,10 @@ int dvm_batch_shape_class(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int* sh
  * class and clears the table.  Setting drops cached plans and graphs. */
 int dvm_ctx_set_pair_config(dvm_ctx* ctx, int shape_class, const dvm_pair_config* cfg);
 int dvm_ctx_get_pair_config(dvm_ctx* ctx, int shape_class, dvm_pair_config* out);
+/* The tuned classes (up to max_entries of them; *count = how many there are), so
+ * a host can persist a table and restore it with dvm_ctx_set_pair_config. */
+int dvm_ctx_tuning_table(dvm_ctx* ctx, int max_entries, int* shape_classes,
+                         dvm_pair_config* cfgs, int* count);
 
 /* ---- serving (no counterpart in the reference) ----------------------------------------
  * A request loop over one context: requests (a body, parameters and a step

@@ -66,3 +66,21 @@ def test_autotune_keeps_the_fastest_for_the_class(ctx):
     ref = _run(ctx)
     for a, b in zip(tuned, ref):
         assert np.array_equal(a["u"], b["u"]) and np.array_equal(a["x"], b["x"])
+
+
+def test_tuning_table_round_trip(ctx, tmp_path):
+    ctx.set_pair_config(7, 128, 2, 1)
+    ctx.set_pair_config(41, 256, 1, 0)
+    table = ctx.tuning_table()
+    assert table[7] == {"tile": 128, "ctas_per_sm": 2, "order": 1}
+    assert table[41] == {"tile": 256, "ctas_per_sm": 1, "order": 0}
+    path = tmp_path / "tuning.json"
+    ctx.save_tuning(str(path))
+    other = N.Context(0)
+    other.load_tuning(str(path))
+    assert other.tuning_table() == table
+    other.close()
+    with pytest.raises(N.DvmError):
+        ctx.set_pair_config(3, 256, 4, 0)  # 256-target items allow 1..3 CTAs per SM
+    ctx.set_pair_config(-1, 256, 3, 0)
+    assert ctx.tuning_table() == {}
