@@ -150,6 +150,8 @@ struct dvm_ctx {
     bool tuning_default_set = false;
     PairConfig tuning_default;
     ListEntry* d_tune_list = nullptr;  // scratch list for the tuner (1024 entries)
+    InstState* h_state = nullptr;      // pinned copy of the state table (batched status)
+    int h_state_slots = 0;
     uint64_t plan_clock = 0;
     ListEntry* list_pool = nullptr;  // kMaxPlans slots of kPoolPerPlan entries
     std::vector<int> pool_free;
@@ -686,6 +688,7 @@ int dvm_ctx_destroy(dvm_ctx* c) {
     if (c->raw_block) cudaFree(c->raw_block);
     if (c->list_pool) cudaFree(c->list_pool);
     if (c->d_tune_list) cudaFree(c->d_tune_list);
+    if (c->h_state) cudaFreeHost(c->h_state);
     if (c->d_table) cudaFree(c->d_table);
     if (c->d_state) cudaFree(c->d_state);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1177,6 +1180,36 @@ int dvm_sim_rng_position(dvm_sim* s, uint64_t* consumed, uint64_t* avail) {
     CK(cudaStreamSynchronize(s->ctx->stream));
     if (consumed) *consumed = s->consumed_base + cursor;
     if (avail) *avail = s->h.ucount - cursor;
+    return DVM_OK;
+}
+
+int dvm_batch_status(dvm_ctx* c, dvm_sim* const* sims, int nsims, int32_t* status) {
+    if (!c || nsims < 0 || (nsims && (!sims || !status))) return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    int hi = 0;
+    for (int i = 0; i < nsims; ++i) {
+        if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        hi = std::max(hi, sims[i]->slot + 1);
+    }
+    if (c->h_state_slots < hi) {
+        if (c->h_state) cudaFreeHost(c->h_state);
+        c->h_state = nullptr;
+        c->h_state_slots = 0;
+        CK(cudaMallocHost(&c->h_state, sizeof(InstState) * (size_t)hi));
+        c->h_state_slots = hi;
+    }
+    CK(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(InstState) * (size_t)hi,
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < nsims; ++i) {
+        const int st = c->h_state[sims[i]->slot].status;
+        status[i] = st == 0 ? DVM_OK
+                  : st == kErrCapacity ? DVM_ERR_CAPACITY
+                  : st == kErrRelease ? DVM_ERR_RELEASE
+                  : st == kErrRngExhausted ? DVM_ERR_RNG : st;
+    }
     return DVM_OK;
 }
 

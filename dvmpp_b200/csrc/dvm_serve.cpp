@@ -160,11 +160,14 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
     uint64_t in_use = 0, peak = 0, ticks = 0, sim_steps = 0;
     uint32_t peak_active = 0;
     std::vector<dvm_sim*> batch;
+    std::vector<int32_t> tick_status;
+    double t_admit = 0.0, t_step = 0.0, t_retire = 0.0;
     while (finished < s->reqs.size()) {
         const double t = now();
         while (next < order.size() && (!realtime || s->reqs[order[next]].arrival <= t))
             waiting.push_back(order[next++]);
         // admission: FIFO while a slot is free and the slab fits the budget
+        const double ta = now();
         while (!waiting.empty() && (int)active.size() < cap_active) {
             Request& r = s->reqs[waiting.front()];
             if (in_use + r.bytes > s->budget) break;
@@ -182,6 +185,7 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
             in_use += r.bytes;
             active.push_back((size_t)r.id);
         }
+        t_admit += now() - ta;
         peak = std::max(peak, in_use);
         peak_active = std::max<uint32_t>(peak_active, (uint32_t)active.size());
         if (active.empty()) {
@@ -196,6 +200,7 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
         // With DVM_SERVE_SYNC each tick is waited for (device status read per
         // simulation); without it the host runs ahead and the status of a
         // simulation is read only when it retires (step counts are host-known).
+        const double tsx = now();
         if (s->autotune) {  // once per new shape class (tuning never changes results)
             int cls = -1;
             int rc = dvm_batch_shape_class(s->ctx, batch.data(), (int)batch.size(), &cls);
@@ -211,18 +216,27 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
         if (rc) return rc;
         ++ticks;
         sim_steps += active.size();
+        if (s->sync_tick) {  // one status copy (and wait) for the whole tick
+            tick_status.resize(batch.size());
+            rc = dvm_batch_status(s->ctx, batch.data(), (int)batch.size(), tick_status.data());
+            if (rc) return rc;
+        }
+        const double tr = now();
+        t_step += tr - tsx;
         // retire: finished (or failed) simulations leave the batch at once
         std::vector<size_t> keep_active;
-        for (size_t i : active) {
+        for (size_t a = 0; a < active.size(); ++a) {
+            const size_t i = active[a];
             Request& r = s->reqs[i];
             r.done += 1;
             int st = DVM_OK;
-            if (s->sync_tick) st = dvm_sim_status(r.sim);
+            if (s->sync_tick) st = tick_status[a];
             if (st == DVM_OK && r.done < r.steps) {
                 keep_active.push_back(i);
                 continue;
             }
             r.status = s->sync_tick ? st : dvm_sim_status(r.sim);
+            if (r.status != DVM_OK) dvm_sim_status(r.sim);  // sets the thread's error message
             dvm_sim_get_loads(r.sim, &r.fx, &r.fz, &r.cd, &r.cl);
             dvm_sim_num_blobs(r.sim, &r.blobs);
             if (s->keep) {
@@ -240,6 +254,7 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
             ++finished;
         }
         active.swap(keep_active);
+        t_retire += now() - tr;
     }
     const double wall = now();
     std::vector<double> lat, queue;
@@ -258,6 +273,10 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
     S.ticks = ticks;
     S.wall_s = wall;
     S.sim_steps_per_s = wall > 0 ? (double)sim_steps / wall : 0.0;
+    S.admit_s = t_admit;
+    S.step_s = t_step;
+    S.retire_s = t_retire;
+    S.tunings = s->tunings;
     S.latency_p50_s = percentile(lat, 0.50);
     S.latency_p95_s = percentile(lat, 0.95);
     S.latency_p99_s = percentile(lat, 0.99);

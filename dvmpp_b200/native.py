@@ -247,6 +247,11 @@ class Context:
                 "default_ms": r.default_ms,
                 "candidates": [dict(c, ms=r.ms[k]) for k, c in enumerate(cands[:r.candidates])]}
 
+    def batch_status(self, sims) -> list:
+        out = (C.c_int32 * max(len(sims), 1))()
+        _check(self.lib.dvm_batch_status(self.h, self._sim_array(sims), len(sims), out))
+        return [int(out[k]) for k in range(len(sims))]
+
     def shape_class(self, sims) -> int:
         v = C.c_int()
         _check(self.lib.dvm_batch_shape_class(self.h, self._sim_array(sims), len(sims),
@@ -445,7 +450,8 @@ class ServerSummary(C.Structure):
                 ("latency_p95_s", C.c_double), ("latency_p99_s", C.c_double),
                 ("latency_mean_s", C.c_double), ("queue_p50_s", C.c_double),
                 ("queue_p99_s", C.c_double), ("peak_active", C.c_uint32),
-                ("peak_bytes", C.c_uint64)]
+                ("peak_bytes", C.c_uint64), ("admit_s", C.c_double), ("step_s", C.c_double),
+                ("retire_s", C.c_double), ("tunings", C.c_uint32)]
 
 
 class PairConfig(C.Structure):
@@ -484,6 +490,7 @@ SIGNATURES.update({
     "dvm_ctx_get_pair_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(PairConfig)]),
     "dvm_ctx_tuning_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                        C.POINTER(PairConfig), C.POINTER(C.c_int)]),
+    "dvm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]),
 })
 
 

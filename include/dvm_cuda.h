@@ -247,6 +247,9 @@ int dvm_sim_step(dvm_sim* sim, int nsteps);
  * of them in one launch.  use_graph != 0 captures the step in a CUDA graph
  * (re-used while the list is unchanged).  Asynchronous: check dvm_sim_status. */
 int dvm_step_batch(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int nsteps, int use_graph);
+/* Device status of every listed simulation with one copy and one wait (what
+ * dvm_sim_status returns, per simulation, into status[i]). */
+int dvm_batch_status(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int32_t* status);
 
 /* ---- pair-kernel autotuning (no counterpart in the reference) ---------------------
  * The FP32 blob-on-blob kernel's launch shape: targets per work item, persistent
@@ -320,6 +323,10 @@ typedef struct {
     double queue_p50_s, queue_p99_s;
     uint32_t peak_active;
     uint64_t peak_bytes;
+    /* host wall time spent admitting (simulation set-up, incl. the QR), issuing
+     * and waiting for ticks, and retiring (results read back); tunings run */
+    double admit_s, step_s, retire_s;
+    uint32_t tunings;
 } dvm_server_summary;
 
 /* hbm_budget_bytes: device memory the server's simulations may hold (0: the

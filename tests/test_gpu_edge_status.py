@@ -54,6 +54,7 @@ def test_capacity_overflow_stops_the_simulation_only(ctx):
     for _ in range(6):
         ctx.step_batch([small, other], 1, use_graph=False)
     assert small.status() == N.ERR_CAPACITY
+    assert ctx.batch_status([small, other]) == [N.ERR_CAPACITY, N.OK]
     n_stop = small.n
     assert 0 < n_stop <= 1024
     ctx.step_batch([small, other], 1, use_graph=False)
