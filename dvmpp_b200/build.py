@@ -92,9 +92,12 @@ def build_oracle(verbose=False) -> None:
     reference's own sources when they are present on this machine."""
     odir = os.path.join(ROOT, "oracle")
     targets = ["oracle"]
-    if os.path.isdir(os.environ.get("DVM_REFERENCE", "/root/reference") + "/src"):
+    ref_present = os.path.isdir(os.environ.get("DVM_REFERENCE", "/root/reference") + "/src")
+    if ref_present:
         targets.append("ref")
     _run(["make", "-s", "-C", odir, *targets], verbose)
+    if ref_present:  # the reference's own C++ tests against the drop-in classes
+        _run(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp")], verbose)
 
 
 def main(argv=None):
