@@ -1682,6 +1682,45 @@ int dvm_biot_savart_at_device(dvm_ctx* c, const double* x, const double* z, cons
     return DVM_OK;
 }
 
+int dvm_sim_probe(dvm_sim* s, const double* px, const double* pz, uint64_t n, double* u,
+                  double* w, double* uvs, double* wvs) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    if (n && (!px || !pz || !u || !w)) return fail(DVM_ERR_ARG, "null probe array");
+    if (n == 0) return DVM_OK;
+    if (n > (1u << 24)) return fail(DVM_ERR_ARG, "too many probe points (max 2^24)");
+    dvm_ctx* c = s->ctx;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    uint32_t ns = 0;
+    CK(cudaMemcpyAsync(&ns, &c->d_state[s->slot].n, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const uint32_t nt = (uint32_t)n;
+    const size_t part_bytes = align_up(16 * direct_at_part_elems(ns, nt), 256);
+    int rc = raw_reserve(c, part_bytes + 8 * 6 * (size_t)n);
+    if (rc) return rc;
+    double* d = reinterpret_cast<double*>(static_cast<char*>(c->raw_block) + part_bytes);
+    double *dx = d, *dz = d + n, *dres = d + 2 * n;  // dres: u, w, uvs, wvs
+    CK(cudaMemcpyAsync(dx, px, 8 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dz, pz, 8 * n, cudaMemcpyHostToDevice, c->stream));
+    // blobs: the at-target sum (pairs closer than r^2 = 1e-15 skipped, as in
+    // src/VelocityKernel.cpp:89), in the simulation's precision
+    direct_at_raw(s->h.x, s->h.z, s->h.circ, s->h.sigma, ns, dx, dz, nt, dres, dres + n,
+                  s->h.precision, 1, static_cast<double2*>(c->raw_block), c->sms, c->stream);
+    sheet_at(s->h, dx, dz, nt, dres + 2 * n, dres + 3 * n, c->stream);
+    g_launches += ns ? 3 : 1;
+    std::vector<double> h(4 * n);
+    CK(cudaMemcpyAsync(h.data(), dres, 8 * 4 * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (uint64_t i = 0; i < n; ++i) {
+        u[i] = (h[i] + h[2 * n + i]) + s->h.ux;
+        w[i] = (h[n + i] + h[3 * n + i]) + s->h.uz;
+        if (uvs) uvs[i] = h[2 * n + i];
+        if (wvs) wvs[i] = h[3 * n + i];
+    }
+    return DVM_OK;
+}
+
 int dvm_biot_savart_at(dvm_ctx* c, const dvm_particle* p, uint64_t ns, const double* tx,
                        const double* tz, uint64_t nt, dvm_velocity* out, int precision) {
     if (!c || (ns && !p) || (nt && (!tx || !tz || !out))) return fail(DVM_ERR_ARG, "null argument");

@@ -187,6 +187,10 @@ void direct_at_raw(const double* x, const double* z, const double* circ, const d
                    double* w, int precision, int skip_close, double2* part, int sms,
                    cudaStream_t s);
 size_t direct_at_part_elems(uint32_t ns, uint32_t nt);
+// Sheet velocity at arbitrary points from one simulation's panels and gamma
+// (the sheet-on-blob sum of src/VortexSheet.cpp:217-273, FP64), for probes.
+void sheet_at(const InstDesc& d, const double* px, const double* pz, uint32_t n, double* uvs,
+              double* wvs, cudaStream_t s);
 
 // gamma = P b (+ refinement), replacing src/VortexSheet.cpp:214.
 void sheet_solve(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,

@@ -217,6 +217,54 @@ __device__ __forceinline__ void sheet_pair_f32(float dx, float dz, float dxe, fl
     ws += (double)fmaf(ay, g0, qy * dg);
 }
 
+// One panel term of src/VortexSheet.cpp:235-249, 261-268 in FP64 with the
+// reference's operation order (one rounding per operation); dx, dz are the
+// point's offsets from the panel's collocation point.
+__device__ __forceinline__ void sheet_pair_f64(double dx, double dz, double dsj, double ct,
+                                               double stt, double c2t, double s2t, double g0,
+                                               double g1, double& us, double& ws) {
+    const double c1 = dsub(dmul(-dx, ct), dmul(dz, stt));
+    const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
+    const double c5 = dsub(dmul(dx, stt), dmul(dz, ct));
+    const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
+    const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
+    const double c8 = dadd(dmul(dx, s2t), dmul(dz, c2t));
+    const double c9 = dsub(dmul(dx, c2t), dmul(dz, s2t));
+    const double qx = dadd(dadd(-stt, ddiv(dmul(dmul(0.5, c8), c6), dsj)),
+                           ddiv(dmul(dadd(dmul(c1, ct), dmul(c5, stt)), c7), dsj));
+    const double px = dsub(dsub(dmul(dmul(-0.5, c6), stt), dmul(c7, ct)), qx);
+    const double qy = dadd(dadd(ct, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
+                           ddiv(dmul(dsub(dmul(c1, stt), dmul(c5, ct)), c7), dsj));
+    const double py = dsub(dsub(dmul(dmul(0.5, c6), ct), dmul(c7, stt)), qy);
+    us = dadd(us, dadd(dmul(px, g0), dmul(qx, g1)));
+    ws = dadd(ws, dadd(dmul(py, g0), dmul(qy, g1)));
+}
+
+// Sheet velocity at arbitrary points (probes): the same panel sum as the
+// sheet-on-blob velocity, over every panel, in FP64; one thread per point.
+__global__ void __launch_bounds__(128) k_sheet_at(const double* __restrict__ xc,
+                                                  const double* __restrict__ zc,
+                                                  const double* __restrict__ ds,
+                                                  const double* __restrict__ cth,
+                                                  const double* __restrict__ sth,
+                                                  const double* __restrict__ c2th,
+                                                  const double* __restrict__ s2th,
+                                                  const double* __restrict__ gamma, int np,
+                                                  const double* __restrict__ px,
+                                                  const double* __restrict__ pz, uint32_t n,
+                                                  double* __restrict__ uvs,
+                                                  double* __restrict__ wvs) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double xi = px[i], zi = pz[i];
+    double us = 0.0, ws = 0.0;
+    for (int j = 0; j < np; ++j)
+        sheet_pair_f64(dsub(xi, xc[j]), dsub(zi, zc[j]), ds[j], cth[j], sth[j], c2th[j], s2th[j],
+                       gamma[j], gamma[j == np - 1 ? 0 : j + 1], us, ws);
+    uvs[i] = dmul(us, kRpi2);
+    wvs[i] = dmul(ws, kRpi2);
+}
+
 __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restrict__ table,
                                                         const InstState* __restrict__ st,
                                                         const ListEntry* __restrict__ list,
@@ -300,26 +348,10 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
                                    (float)(xi - sex[j]), (float)(zi - sez[j]), fpan[j], fg[j],
                                    fdg[j], us, ws);
             } else {
-                for (int j = 0; j < np; ++j) {
-                    const double dsj = sds[j], ct = sct[j], stt = sst[j];
-                    const double dx = dsub(xi, sxc[j]), dz = dsub(zi, szc[j]);
-                    const double c1 = dsub(dmul(-dx, ct), dmul(dz, stt));
-                    const double c2 = dadd(dmul(dx, dx), dmul(dz, dz));
-                    const double c5 = dsub(dmul(dx, stt), dmul(dz, ct));
-                    const double c6 = log(dadd(1.0, dmul(dsj, ddiv(dadd(dsj, dmul(2.0, c1)), c2))));
-                    const double c7 = atan2(dmul(c5, dsj), dadd(c2, dmul(c1, dsj)));
-                    const double c8 = dadd(dmul(dx, ss2[j]), dmul(dz, sc2[j]));
-                    const double c9 = dsub(dmul(dx, sc2[j]), dmul(dz, ss2[j]));
-                    const double qx = dadd(dadd(-stt, ddiv(dmul(dmul(0.5, c8), c6), dsj)),
-                                           ddiv(dmul(dadd(dmul(c1, ct), dmul(c5, stt)), c7), dsj));
-                    const double px = dsub(dsub(dmul(dmul(-0.5, c6), stt), dmul(c7, ct)), qx);
-                    const double qy = dadd(dadd(ct, ddiv(dmul(dmul(0.5, c9), c6), dsj)),
-                                           ddiv(dmul(dsub(dmul(c1, stt), dmul(c5, ct)), c7), dsj));
-                    const double py = dsub(dsub(dmul(dmul(0.5, c6), ct), dmul(c7, stt)), qy);
-                    const double g0 = sg[j], g1 = (j == np - 1) ? sg[0] : sg[j + 1];
-                    us = dadd(us, dadd(dmul(px, g0), dmul(qx, g1)));
-                    ws = dadd(ws, dadd(dmul(py, g0), dmul(qy, g1)));
-                }
+                for (int j = 0; j < np; ++j)
+                    sheet_pair_f64(dsub(xi, sxc[j]), dsub(zi, szc[j]), sds[j], sct[j], sst[j],
+                                   sc2[j], ss2[j], sg[j], (j == np - 1) ? sg[0] : sg[j + 1], us,
+                                   ws);
             }
             const double uvs = dmul(us, kRpi2), wvs = dmul(ws, kRpi2);
             d.uvs[i] = uvs;
@@ -471,6 +503,13 @@ void sheet_velocity(const InstDesc* table, InstState* st, const ListEntry* list,
     }
     cudaMemsetAsync(ws.work + 1, 0, sizeof(unsigned), s);
     k_sheet_velocity<<<sms * 4, 256, smem, s>>>(table, st, list, nlist, mode, ws.work + 1);
+}
+
+void sheet_at(const InstDesc& d, const double* px, const double* pz, uint32_t n, double* uvs,
+              double* wvs, cudaStream_t s) {
+    if (n == 0) return;
+    k_sheet_at<<<(n + 127) / 128, 128, 0, s>>>(d.xc, d.zc, d.ds, d.cth, d.sth, d.c2th, d.s2th,
+                                               d.gamma, d.np, px, pz, n, uvs, wvs);
 }
 
 void convect_update(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,

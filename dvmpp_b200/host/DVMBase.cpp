@@ -105,25 +105,46 @@ void DVMBase::convect() { dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_CONVE
 
 void DVMBase::remesh() {}
 
-void DVMBase::sync_to_host() {
+// full: every blob array (what a caller reads after run()); otherwise only
+// what the output files need (positions, circulations, the sheet and loads).
+void DVMBase::sync_to_host(bool full) {
     uint64_t n = 0;
     dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "DVMBase");
     m_vortex.resize((unsigned)n);
-    std::vector<uint32_t> ids(n);
-    dvm::check_status(
-        dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(m_vortex.m_x), dvm::vec_ptr(m_vortex.m_z),
-                          dvm::vec_ptr(m_vortex.m_circ), dvm::vec_ptr(m_vortex.m_sigma),
-                          dvm::vec_ptr(m_vortex.m_u), dvm::vec_ptr(m_vortex.m_w),
-                          dvm::vec_ptr(m_vortex.m_uvs), dvm::vec_ptr(m_vortex.m_wvs), ids.data()),
-        "DVMBase");
-    for (uint64_t i = 0; i < n; ++i) m_vortex.m_ID[i] = ids[i];
+    if (full) {
+        std::vector<uint32_t> ids(n);
+        dvm::check_status(
+            dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(m_vortex.m_x), dvm::vec_ptr(m_vortex.m_z),
+                              dvm::vec_ptr(m_vortex.m_circ), dvm::vec_ptr(m_vortex.m_sigma),
+                              dvm::vec_ptr(m_vortex.m_u), dvm::vec_ptr(m_vortex.m_w),
+                              dvm::vec_ptr(m_vortex.m_uvs), dvm::vec_ptr(m_vortex.m_wvs),
+                              ids.data()),
+            "DVMBase");
+        for (uint64_t i = 0; i < n; ++i) m_vortex.m_ID[i] = ids[i];
+    } else {
+        dvm::check_status(dvm_sim_get_blobs(m_sim, n, &n, dvm::vec_ptr(m_vortex.m_x),
+                                            dvm::vec_ptr(m_vortex.m_z),
+                                            dvm::vec_ptr(m_vortex.m_circ), nullptr, nullptr,
+                                            nullptr, nullptr, nullptr, nullptr),
+                          "DVMBase");
+    }
     m_vortsheet.pull_from_device();
 }
 
 void DVMBase::write_outputs() {
-    m_vortex.write_step(m_time, m_step);
-    m_vortsheet.write_step(m_time);
-    m_probe.write_step(m_time);
+    if (m_probe.size())  // velocities at the probe points from the device-resident state
+        dvm::check_status(dvm_sim_probe(m_sim, dvm::vec_ptr(m_probe.m_x),
+                                        dvm::vec_ptr(m_probe.m_z), m_probe.size(),
+                                        dvm::vec_ptr(m_probe.m_u), dvm::vec_ptr(m_probe.m_w),
+                                        dvm::vec_ptr(m_probe.m_uvs), dvm::vec_ptr(m_probe.m_wvs)),
+                          "DVMBase probes");
+    // one job per step, so the files are appended step by step in order
+    m_writer.submit([a = m_vortex.write_step_job(m_time, m_step),
+                     b = m_vortsheet.write_step_job(m_time), c = m_probe.write_step_job(m_time)] {
+        a();
+        b();
+        c();
+    });
 }
 
 void DVMBase::run(unsigned steps, bool write, bool quiet) {
@@ -131,7 +152,8 @@ void DVMBase::run(unsigned steps, bool write, bool quiet) {
     for (unsigned j = 1; j <= steps; j++) {
         increment_step();
         compute_step();
-        if (write || !quiet || j == steps) sync_to_host();
+        if (j == steps) sync_to_host(true);
+        else if (write || !quiet) sync_to_host(false);
         if (write) write_outputs();
         if (!quiet) {
             double fx = 0, fz = 0, cd = 0, cl = 0;
@@ -142,6 +164,7 @@ void DVMBase::run(unsigned steps, bool write, bool quiet) {
             std::cout << "Number of vortex blobs   = " << m_vortex.size() << std::endl;
         }
     }
+    m_writer.flush();  // every file complete on return
 }
 
 void DVMBase::solve() { run(get_steps(), true, false); }

@@ -2,7 +2,8 @@
 // and solve().  The time loop keeps every blob and the sheet on the GPU
 // (one device-resident simulation, one batched kernel sequence per step) and
 // copies state back only for the per-step output files, which keep the
-// reference's formats.  The random walk uses the reference's stream
+// reference's formats and are written by a background thread (the files are
+// complete when solve() / run() return).  The random walk uses the reference's stream
 // (constants/seed through std::mt19937) unless algorithms/diffusion_rng is
 // "philox".  algorithms/velocity_kernel selects the pair arithmetic:
 // "direct" (default, FP64) or "cuda" (FP32 with compensated sums).
@@ -13,6 +14,7 @@
 
 #include "BaseTypes.hpp"
 #include "Exceptions.hpp"
+#include "OutputWriter.hpp"
 #include "Probe.hpp"
 #include "Random.hpp"
 #include "VortexBlobs.hpp"
@@ -38,6 +40,10 @@ class DVMBase
     int m_precision = DVM_F64;
     bool m_quiet = false;
     dvm_sim* m_sim = nullptr;  // owned by m_vortsheet
+    // Output files are formatted and appended on a background thread while
+    // the GPU runs the next step (declared last: destroyed, i.e. drained,
+    // before the objects its jobs were copied from).
+    dvm::AsyncWriter m_writer{2};
 
     void compute_step();
     void increment_step();
@@ -46,7 +52,7 @@ class DVMBase
     void convect();
     void remesh();
     void write_outputs();
-    void sync_to_host();
+    void sync_to_host(bool full = true);
     void supply_uniforms();
 
   public:

@@ -4,6 +4,7 @@
 #include <fstream>
 
 #include "Exceptions.hpp"
+#include "OutputWriter.hpp"
 
 namespace fs = std::filesystem;
 
@@ -29,8 +30,18 @@ Probe::Probe(const XmlHandler& xml, const std::string& stamp) {
 
 unsigned Probe::size() const { return static_cast<unsigned>(m_x.n_elem); }
 
-void Probe::write_step(double time) {
-    std::ofstream of(m_outfile, std::ios_base::app);
-    if (!of) throw dvm::FileIOException::cannotWrite(m_outfile);
-    for (unsigned i = 0; i < size(); ++i) of << time << "\t" << m_u(i) << "\t" << m_w(i) << "\n";
+void Probe::write_step(double time) { write_step_job(time)(); }
+
+std::function<void()> Probe::write_step_job(double time) const {
+    // format of src/Probe.cpp:43-55: "t u w" per probe point
+    std::string s;
+    for (unsigned i = 0; i < size(); ++i) {
+        dvm::append_g(s, time);
+        s += '\t';
+        dvm::append_g(s, m_u(i));
+        s += '\t';
+        dvm::append_g(s, m_w(i));
+        s += '\n';
+    }
+    return [s = std::move(s), path = m_outfile] { dvm::append_file(path, s); };
 }

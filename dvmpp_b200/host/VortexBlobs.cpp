@@ -3,8 +3,10 @@
 #include <filesystem>
 #include <fstream>
 #include <iostream>
+#include <thread>
 
 #include "Device.hpp"
+#include "OutputWriter.hpp"
 #include "VelocityKernel.hpp"
 
 namespace fs = std::filesystem;
@@ -157,14 +159,25 @@ void VortexBlobs::print_circulation() const {
     for (unsigned i = 0; i < size(); ++i) std::cout << " circ = " << m_circ(i) << std::endl;
 }
 
-void VortexBlobs::write_step(double time, unsigned step) {
+void VortexBlobs::write_step(double time, unsigned step) { write_step_job(time, step)(); }
+
+std::function<void()> VortexBlobs::write_step_job(double time, unsigned step) const {
+    // formats of src/VortexBlobs.cpp:310-332: one "t x z circ" row per blob,
+    // then "step n" in the count file
     if (m_blobsfile.empty() || m_numfile.empty())
         throw dvm::FileIOException("VortexBlobs::write_step: must set filenames before writing");
-    std::ofstream bf(m_blobsfile, std::ios_base::app);
-    if (!bf) throw dvm::FileIOException::cannotWrite(m_blobsfile);
-    for (unsigned i = 0; i < size(); ++i)
-        bf << time << "\t" << m_x(i) << "\t" << m_z(i) << "\t" << m_circ(i) << "\n";
-    std::ofstream nf(m_numfile, std::ios_base::app);
-    if (!nf) throw dvm::FileIOException::cannotWrite(m_numfile);
-    nf << step << "\t" << size() << "\n";
+    const size_t n = size();
+    std::vector<double> x(m_x.memptr(), m_x.memptr() + n), z(m_z.memptr(), m_z.memptr() + n),
+        c(m_circ.memptr(), m_circ.memptr() + n);
+    return [time, step, n, x = std::move(x), z = std::move(z), c = std::move(c),
+            bfile = m_blobsfile, nfile = m_numfile] {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency() / 2);
+        dvm::append_file(bfile, dvm::format_rows4(time, x.data(), z.data(), c.data(), n, hw));
+        std::string line;
+        dvm::append_u(line, step);
+        line += '\t';
+        dvm::append_u(line, n);
+        line += '\n';
+        dvm::append_file(nfile, line);
+    };
 }

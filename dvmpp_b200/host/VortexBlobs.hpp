@@ -7,6 +7,7 @@
 #ifndef DVMPP_B200_VORTEXBLOBS_HPP
 #define DVMPP_B200_VORTEXBLOBS_HPP
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -57,6 +58,9 @@ class VortexBlobs
     void print_velocity() const;
     void print_circulation() const;
     void write_step(double time, unsigned step);
+    // The same output as a job that owns copies of what it writes (for a
+    // background writer; files are appended when the job runs).
+    [[nodiscard]] std::function<void()> write_step_job(double time, unsigned step) const;
     void setKernelType(const std::string& type);
     [[nodiscard]] std::string kernelType() const;
     void copyOutputConfig(const VortexBlobs& other);

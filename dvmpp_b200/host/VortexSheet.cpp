@@ -1,5 +1,8 @@
 #include "VortexSheet.hpp"
 
+#include "OutputWriter.hpp"
+#include "Probe.hpp"
+
 #include <algorithm>
 #include <cmath>
 #include <filesystem>
@@ -40,18 +43,18 @@ VortexSheet::VortexSheet(const XmlHandler& xml, const std::string& stamp) {
     build_device((uint64_t)(steps * 2.0 * (m_maxNumPanelVort + 1) * npanels) + 4096);
 
     const std::string outdir = xml.getStringAttribute("io", "output_dir", true);
-    const auto gamma_path = fs::path(outdir) / (stamp + "_gamma.dat");
-    m_gammafile.open(gamma_path);
-    if (!m_gammafile) throw dvm::FileIOException::cannotOpen(gamma_path.string());
+    m_gammapath = (fs::path(outdir) / (stamp + "_gamma.dat")).string();
+    std::ofstream gammafile(m_gammapath);
+    if (!gammafile) throw dvm::FileIOException::cannotOpen(m_gammapath);
     // headers of src/VortexSheet.cpp:43-53
-    m_gammafile << m_xc.n_elem << " # Number of collocation points\n"
-                << m_dt << " # Time Step\n"
-                << steps << " # Steps\n"
-                << "Time [s] Gamma - Vortex sheet strength\n";
-    const auto force_path = fs::path(outdir) / (stamp + "_loads.dat");
-    m_forcefile.open(force_path);
-    if (!m_forcefile) throw dvm::FileIOException::cannotOpen(force_path.string());
-    m_forcefile << "Time [s]\tF_x [-]\tF_z [s]\n";
+    gammafile << m_xc.n_elem << " # Number of collocation points\n"
+              << m_dt << " # Time Step\n"
+              << steps << " # Steps\n"
+              << "Time [s] Gamma - Vortex sheet strength\n";
+    m_forcepath = (fs::path(outdir) / (stamp + "_loads.dat")).string();
+    std::ofstream forcefile(m_forcepath);
+    if (!forcefile) throw dvm::FileIOException::cannotOpen(m_forcepath);
+    forcefile << "Time [s]\tF_x [-]\tF_z [s]\n";
 }
 
 VortexSheet::~VortexSheet() {
@@ -136,7 +139,7 @@ unsigned VortexSheet::max_release() const {
     return 16u * (m_maxNumPanelVort + 1) * size() + 1024u;
 }
 
-void VortexSheet::upload(VortexBlobs& b) {
+void VortexSheet::upload(const VortexBlobs& b) {
     const unsigned n = b.size();
     device((uint64_t)n + max_release());
     dvm::check_status(dvm_sim_set_blobs(m_sim, n, dvm::vec_ptr(b.m_x), dvm::vec_ptr(b.m_z),
@@ -270,16 +273,47 @@ void VortexSheet::print_gamma() const {
     for (size_t i = 0; i < m_gamma.n_elem; ++i) std::cout << "   " << m_gamma(i) << "\n";
 }
 
-void VortexSheet::write_step(double time) {
+void VortexSheet::write_step(double time) { write_step_job(time)(); }
+
+std::function<void()> VortexSheet::write_step_job(double time) const {
     // formats of src/VortexSheet.cpp:335-343
-    for (size_t i = 0; i < m_xc.n_elem; ++i)
-        m_gammafile << time << "\t " << m_xc(i) << "\t" << m_zc(i) << "\t" << m_gamma(i) << "\t"
-                    << m_ds(i) << "\n";
-    m_forcefile << time << "\t" << m_fx << "\t" << m_fz << "\n";
+    if (m_gammapath.empty() || m_forcepath.empty())
+        throw dvm::FileIOException("VortexSheet::write_step: no output files were set up");
+    std::string g, f;
+    for (size_t i = 0; i < m_xc.n_elem; ++i) {
+        dvm::append_g(g, time);
+        g += "\t ";
+        dvm::append_g(g, m_xc(i));
+        g += '\t';
+        dvm::append_g(g, m_zc(i));
+        g += '\t';
+        dvm::append_g(g, m_gamma(i));
+        g += '\t';
+        dvm::append_g(g, m_ds(i));
+        g += '\n';
+    }
+    dvm::append_g(f, time);
+    f += '\t';
+    dvm::append_g(f, m_fx);
+    f += '\t';
+    dvm::append_g(f, m_fz);
+    f += '\n';
+    return [g = std::move(g), f = std::move(f), gp = m_gammapath, fp = m_forcepath] {
+        dvm::append_file(gp, g);
+        dvm::append_file(fp, f);
+    };
 }
 
 std::tuple<double, double> VortexSheet::get_forces() const { return std::make_tuple(m_fx, m_fz); }
 
-void VortexSheet::probe_velocities(const VortexBlobs&, Probe&) {
-    throw dvm::AlgorithmException("VortexSheet::probe_velocities is not provided by this build");
+void VortexSheet::probe_velocities(const VortexBlobs& blobs, Probe& probe) {
+    // The intended formula of src/VortexSheet.cpp:559-646 (blob sum over all
+    // blobs, sheet sum over all panels, free stream), on the GPU.
+    upload(blobs);
+    const unsigned n = probe.size();
+    for (Vector* v : {&probe.m_u, &probe.m_w, &probe.m_uvs, &probe.m_wvs}) v->set_size(n);
+    dvm::check_status(dvm_sim_probe(m_sim, dvm::vec_ptr(probe.m_x), dvm::vec_ptr(probe.m_z), n,
+                                    dvm::vec_ptr(probe.m_u), dvm::vec_ptr(probe.m_w),
+                                    dvm::vec_ptr(probe.m_uvs), dvm::vec_ptr(probe.m_wvs)),
+                      "VortexSheet::probe_velocities");
 }

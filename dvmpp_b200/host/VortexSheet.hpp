@@ -8,6 +8,7 @@
 #define DVMPP_B200_VORTEXSHEET_HPP
 
 #include <fstream>
+#include <functional>
 #include <string>
 #include <tuple>
 
@@ -30,14 +31,14 @@ class VortexSheet
     double m_cutoff_exp = 0.0;
     double m_fx = 0.0, m_fz = 0.0;
     double m_Ux = 0.0, m_Uz = 0.0;
-    std::ofstream m_gammafile, m_forcefile;
+    std::string m_gammapath, m_forcepath;  // output files (headers written at set-up)
     // device side
     dvm_sim_params m_params{};
     dvm_sim* m_sim = nullptr;
 
     void read_input_coord(const std::string& domain);
     void build_device(uint64_t capacity);
-    void upload(VortexBlobs& blobs);
+    void upload(const VortexBlobs& blobs);
 
   public:
     VortexSheet();
@@ -57,6 +58,8 @@ class VortexSheet
     void print_unit_vectors() const;
     void print_gamma() const;
     void write_step(double time);
+    // The same output as a job owning copies of what it writes.
+    [[nodiscard]] std::function<void()> write_step_job(double time) const;
     [[nodiscard]] std::tuple<double, double> get_forces() const;
     // Not provided: the reference never calls it and its formula is not the
     // intended one; throws dvm::AlgorithmException.

@@ -422,6 +422,14 @@ class Simulation:
     def check(self):
         _check(self.lib.dvm_sim_status(self.h))
 
+    def probe(self, px, pz):
+        """Velocity at probe points: (u, w, uvs, wvs) with u, w the total."""
+        px, pz = _f64(px), _f64(pz)
+        n = px.size
+        out = [np.empty(n) for _ in range(4)]
+        _check(self.lib.dvm_sim_probe(self.h, _p(px), _p(pz), n, *[_p(a) for a in out]))
+        return tuple(out)
+
     def clear_status(self):
         _check(self.lib.dvm_sim_clear_status(self.h))
 
@@ -491,6 +499,7 @@ SIGNATURES.update({
     "dvm_ctx_tuning_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                        C.POINTER(PairConfig), C.POINTER(C.c_int)]),
     "dvm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]),
+    "dvm_sim_probe": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]),
 })
 
 

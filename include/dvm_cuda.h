@@ -241,6 +241,16 @@ int dvm_sim_status(dvm_sim* sim);
 int dvm_sim_clear_status(dvm_sim* sim);
 int dvm_sim_phase(dvm_sim* sim, int phase);
 int dvm_sim_step(dvm_sim* sim, int nsteps);
+/* Velocity at probe points (host arrays, n of them) from the simulation's
+ * current blobs, sheet and free stream: the intended formula of
+ * VortexSheet::probe_velocities (src/VortexSheet.cpp:559-646), i.e. what a
+ * blob at the point would be convected with -- (1/2pi) sum over all blobs
+ * (pairs with r^2 <= 1e-15 skipped, as computeInducedAt) + the sheet's
+ * velocity summed over all panels + (ux, uz).  The reference's loop skips
+ * blob 0 and panel 0, keeps only the last panel's term and flips a sign; those
+ * slips are not reproduced.  uvs / wvs (may be null) receive the sheet part. */
+int dvm_sim_probe(dvm_sim* sim, const double* px, const double* pz, uint64_t n, double* u,
+                  double* w, double* uvs, double* wvs);
 
 /* ---- batches ---------------------------------------------------------------------- */
 /* Advance every listed simulation by nsteps; each kernel of the step serves all
