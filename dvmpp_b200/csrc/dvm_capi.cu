@@ -1682,6 +1682,118 @@ int dvm_biot_savart_at_device(dvm_ctx* c, const double* x, const double* z, cons
     return DVM_OK;
 }
 
+// ---- remeshing -------------------------------------------------------------------------
+static int remesh_grid_of(const dvm_remesh_params* p, RemeshGrid* g) {
+    if (!p) return fail(DVM_ERR_ARG, "remesh parameters are null");
+    if (!(p->dx > 0) || !(p->dz > 0)) return fail(DVM_ERR_ARG, "remesh dx, dz must be > 0");
+    if (!(p->xmax >= p->xmin) || !(p->zmax >= p->zmin))
+        return fail(DVM_ERR_ARG, "remesh bounds: need xmax >= xmin and zmax >= zmin");
+    if (p->kernel < DVM_REMESH_M4PRIME || p->kernel > DVM_REMESH_GAUSSIAN)
+        return fail(DVM_ERR_ARG, "unknown remesh kernel");
+    const double fx = std::floor((p->xmax - p->xmin) / p->dx + 1e-9);
+    const double fz = std::floor((p->zmax - p->zmin) / p->dz + 1e-9);
+    if (!(fx < 65535.0) || !(fz < 65535.0) || (fx + 1.0) * (fz + 1.0) > (double)(1u << 28))
+        return fail(DVM_ERR_ARG, "remesh mesh too large (at most 2^28 nodes)");
+    g->x0 = p->xmin;
+    g->z0 = p->zmin;
+    g->dx = p->dx;
+    g->dz = p->dz;
+    g->sigma = p->sigma;
+    g->threshold = p->circ_threshold;
+    g->nx = (int)fx + 1;
+    g->nz = (int)fz + 1;
+    g->kernel = p->kernel;
+    return DVM_OK;
+}
+
+int dvm_remesh_grid(const dvm_remesh_params* p, uint32_t* nx, uint32_t* nz) {
+    RemeshGrid g;
+    const int rc = remesh_grid_of(p, &g);
+    if (rc) return rc;
+    if (nx) *nx = (uint32_t)g.nx;
+    if (nz) *nz = (uint32_t)g.nz;
+    return DVM_OK;
+}
+
+int dvm_sim_remesh(dvm_sim* s, const dvm_remesh_params* p, uint64_t* n_out) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    RemeshGrid g;
+    int rc = remesh_grid_of(p, &g);
+    if (rc) return rc;
+    dvm_ctx* c = s->ctx;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        CK(cudaSetDevice(c->device));
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, &c->d_state[s->slot].n, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        void* scratch = nullptr;
+        const cudaError_t e =
+            pool_alloc(c, &scratch, remesh_scratch_bytes(g, n, s->h.cap));
+        if (e != cudaSuccess)
+            return fail(DVM_ERR_OOM, std::string("remesh scratch: ") + cudaGetErrorString(e));
+        const InstDesc& h = s->h;
+        RemeshDest d{h.x, h.z, h.circ, h.sigma, h.u, h.w, h.uvs, h.wvs, h.id,
+                     &c->d_state[s->slot].n, nullptr};
+        remesh_run(g, h.x, h.z, h.circ, h.sigma, n, h.cap, d, &c->d_state[s->slot].status,
+                   scratch, c->sms, c->stream);
+        pool_free(c, scratch);
+        g_launches += 7;
+        CK(cudaGetLastError());
+    }
+    rc = dvm_sim_status(s);
+    if (rc) return rc;
+    if (n_out) return dvm_sim_num_blobs(s, n_out);
+    return DVM_OK;
+}
+
+int dvm_remesh(dvm_ctx* c, const dvm_particle* in, uint64_t n, const dvm_remesh_params* p,
+               dvm_particle* out, uint64_t out_cap, uint64_t* n_out) {
+    if (!c || (n && !in) || (out_cap && !out) || !n_out) return fail(DVM_ERR_ARG, "null argument");
+    if (n > 0xF0000000ull || out_cap > 0xF0000000ull) return fail(DVM_ERR_ARG, "too many blobs");
+    RemeshGrid g;
+    int rc = remesh_grid_of(p, &g);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    const size_t data = align_up(8 * 4 * (size_t)n, 256) + align_up(8 * 4 * (size_t)out_cap, 256) + 256;
+    rc = raw_reserve(c, data);
+    if (rc) return rc;
+    char* base = static_cast<char*>(c->raw_block);
+    double* din = reinterpret_cast<double*>(base);
+    double* dout = reinterpret_cast<double*>(base + align_up(8 * 4 * (size_t)n, 256));
+    uint32_t* dneed = reinterpret_cast<uint32_t*>(base + data - 256);
+    std::vector<double> h(4 * n);
+    for (uint64_t i = 0; i < n; ++i) {
+        h[i] = in[i].x;
+        h[n + i] = in[i].z;
+        h[2 * n + i] = in[i].circ;
+        h[3 * n + i] = in[i].sigma;
+    }
+    if (n) CK(cudaMemcpyAsync(din, h.data(), 8 * 4 * n, cudaMemcpyHostToDevice, c->stream));
+    void* scratch = nullptr;
+    const cudaError_t e = pool_alloc(c, &scratch, remesh_scratch_bytes(g, (uint32_t)n, (uint32_t)out_cap));
+    if (e != cudaSuccess) return fail(DVM_ERR_OOM, std::string("remesh scratch: ") + cudaGetErrorString(e));
+    RemeshDest d{dout, dout + out_cap, dout + 2 * out_cap, dout + 3 * out_cap, nullptr, nullptr,
+                 nullptr, nullptr, nullptr, nullptr, dneed};
+    remesh_run(g, din, din + n, din + 2 * n, din + 3 * n, (uint32_t)n, (uint32_t)out_cap, d,
+               nullptr, scratch, c->sms, c->stream);
+    pool_free(c, scratch);
+    g_launches += 7;
+    uint32_t need = 0;
+    CK(cudaMemcpyAsync(&need, dneed, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *n_out = need;
+    if (need > out_cap)
+        return fail(DVM_ERR_CAPACITY, "remesh: " + std::to_string(need) + " blobs do not fit out_cap");
+    std::vector<double> r(4 * (size_t)out_cap);
+    if (need) CK(cudaMemcpy(r.data(), dout, 8 * 4 * (size_t)out_cap, cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < need; ++i)
+        out[i] = dvm_particle{r[i], r[out_cap + i], r[2 * out_cap + i], r[3 * out_cap + i]};
+    return DVM_OK;
+}
+
 int dvm_sim_probe(dvm_sim* s, const double* px, const double* pz, uint64_t n, double* u,
                   double* w, double* uvs, double* wvs) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");

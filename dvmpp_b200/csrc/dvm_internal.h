@@ -187,6 +187,24 @@ void direct_at_raw(const double* x, const double* z, const double* circ, const d
                    double* w, int precision, int skip_close, double2* part, int sms,
                    cudaStream_t s);
 size_t direct_at_part_elems(uint32_t ns, uint32_t nt);
+// Remeshing onto a background mesh (k_remesh.cu).  Nodes are x0 + i dx,
+// z0 + j dz for i < nx, j < nz.
+enum RemeshKernel : int { kRemeshM4p = 0, kRemeshM6 = 1, kRemeshGauss = 2 };
+struct RemeshGrid {
+    double x0, z0, dx, dz, sigma, threshold;
+    int nx, nz, kernel;
+};
+struct RemeshDest {  // where the new blob set goes (u..id may be null)
+    double *x, *z, *circ, *sigma, *u, *w, *uvs, *wvs;
+    uint32_t* id;
+    uint32_t* n;     // new count, written only when it fits the capacity
+    uint32_t* need;  // new count, always (may be null)
+};
+size_t remesh_scratch_bytes(const RemeshGrid& g, uint32_t n, uint32_t cap);
+void remesh_run(const RemeshGrid& g, const double* x, const double* z, const double* circ,
+                const double* sigma, uint32_t n, uint32_t cap, const RemeshDest& dest,
+                int* status, void* scratch, int sms, cudaStream_t s);
+
 // Sheet velocity at arbitrary points from one simulation's panels and gamma
 // (the sheet-on-blob sum of src/VortexSheet.cpp:217-273, FP64), for probes.
 void sheet_at(const InstDesc& d, const double* px, const double* pz, uint32_t n, double* uvs,

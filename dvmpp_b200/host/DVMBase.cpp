@@ -7,7 +7,8 @@
 #include "Device.hpp"
 
 DVMBase::DVMBase(XmlHandler& xml, const std::string& stamp)
-    : m_vortex(xml, stamp), m_vortsheet(xml, stamp), m_probe(xml, stamp), m_xml(xml) {
+    : m_vortex(xml, stamp), m_vortsheet(xml, stamp), m_probe(xml, stamp), m_xml(xml),
+      m_mesh(xml) {
     m_nu = xml.getValueAttribute("constants", "nu");
     m_dt = xml.getValueAttribute("time", "dt");
     m_steps = static_cast<unsigned>(xml.getValueAttribute("time", "steps"));
@@ -33,8 +34,9 @@ DVMBase::DVMBase(XmlHandler& xml, const std::string& stamp)
     if (xml.has("algorithms", "merge_frequency") && xml.getValueAttribute("algorithms", "merge_frequency") > 0)
         std::cout << "Vortex merging is not part of this build; merge options are ignored"
                   << std::endl;
-    if (xml.has("remesh", "frequency"))
-        std::cout << "Remeshing is not part of this build; <remesh> is ignored" << std::endl;
+    if (m_mesh.is_enabled())  // as src/DVMBase.cpp:61-64 reports merging
+        std::cout << "Remeshing enabled: " << m_mesh.nx() << " x " << m_mesh.nz()
+                  << " mesh nodes" << std::endl;
     const int cross = m_surfcross == SurfaceCross::Delete
                           ? DVM_DELETE
                           : (m_surfcross == SurfaceCross::Absorb ? DVM_ABSORB : DVM_REFLECT);
@@ -71,7 +73,10 @@ void DVMBase::compute_step() {
     // not-yet-consumed part of the random stream).
     uint64_t n = 0;
     dvm::check_status(dvm_sim_num_blobs(m_sim, &n), "DVMBase");
-    const uint64_t need = n + m_vortsheet.max_release();
+    const bool remesh_now = m_mesh.should_remesh(m_step);
+    // a remesh can turn the blobs into as many blobs as there are mesh nodes
+    const uint64_t need = n + m_vortsheet.max_release() +
+                          (remesh_now ? (uint64_t)m_mesh.nx() * m_mesh.nz() : 0);
     if (need > m_vortsheet.capacity()) {
         std::vector<double> pending;
         if (m_rng_mode == DVM_RNG_INJECT) {
@@ -95,15 +100,29 @@ void DVMBase::compute_step() {
                               "DVMBase");
     }
     supply_uniforms();
-    // convect (Euler or RK3), remesh (off), diffusion, release + append,
-    // surface crossing, loads: src/DVMBase.cpp:86-133, one batched sequence
-    dvm::check_status(dvm_sim_step(m_sim, 1), "DVMBase::compute_step");
+    if (!remesh_now) {
+        // convect (Euler or RK3), diffusion, release + append, surface
+        // crossing, loads: src/DVMBase.cpp:86-133, one batched sequence
+        dvm::check_status(dvm_sim_step(m_sim, 1), "DVMBase::compute_step");
+    } else {
+        // the same step phase by phase, with the remesh after convection
+        // (src/DVMBase.cpp:88-92)
+        for (int ph : {DVM_PHASE_INCREMENT, DVM_PHASE_CONVECT})
+            dvm::check_status(dvm_sim_phase(m_sim, ph), "DVMBase::compute_step");
+        dvm::check_status(dvm_sim_remesh(m_sim, &m_mesh.params(), nullptr), "DVMBase::remesh");
+        supply_uniforms();  // the walk draws 2 per blob of the remeshed set
+        for (int ph : {DVM_PHASE_DIFFUSE, DVM_PHASE_RELEASE, DVM_PHASE_CROSS, DVM_PHASE_LOADS})
+            dvm::check_status(dvm_sim_phase(m_sim, ph), "DVMBase::compute_step");
+    }
     dvm::check_status(dvm_sim_status(m_sim), "DVMBase::compute_step");
 }
 
 void DVMBase::convect() { dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_CONVECT), "convect"); }
 
-void DVMBase::remesh() {}
+void DVMBase::remesh() {
+    if (m_mesh.should_remesh(m_step))
+        dvm::check_status(dvm_sim_remesh(m_sim, &m_mesh.params(), nullptr), "DVMBase::remesh");
+}
 
 // full: every blob array (what a caller reads after run()); otherwise only
 // what the output files need (positions, circulations, the sheet and loads).

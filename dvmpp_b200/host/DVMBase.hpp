@@ -12,6 +12,7 @@
 
 #include <string>
 
+#include "BackgroundMesh.hpp"
 #include "BaseTypes.hpp"
 #include "Exceptions.hpp"
 #include "OutputWriter.hpp"
@@ -32,6 +33,7 @@ class DVMBase
     Probe m_probe;
     Random m_rand;
     XmlHandler m_xml;
+    BackgroundMesh m_mesh;
     double m_nu = 0, m_Ux = 0, m_Uz = 0, m_Ur = 0, m_dt = 0, m_time = 0;
     unsigned m_step = 0, m_steps = 0;
     Scheme m_scheme = Scheme::Euler;

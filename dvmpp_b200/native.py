@@ -227,6 +227,22 @@ class Context:
         v = np.frombuffer(out, dtype=np.float64, count=2 * nt).reshape(nt, 2) if nt else np.zeros((0, 2))
         return v[:, 0].copy(), v[:, 1].copy()
 
+    def remesh(self, x, z, circ, sigma, params: RemeshParams, out_cap=None):
+        """Remesh host arrays (the BackgroundMesh::remesh path): (x, z, circ, sigma)."""
+        n = len(x)
+        p = (Particle * max(n, 1))()
+        if n:
+            arr = np.frombuffer(p, dtype=np.float64, count=4 * n).reshape(n, 4)
+            arr[:, 0], arr[:, 1], arr[:, 2], arr[:, 3] = x, z, circ, sigma
+        if out_cap is None:
+            nx, nz = remesh_grid(params)
+            out_cap = nx * nz + n
+        out = (Particle * max(out_cap, 1))()
+        m = C.c_uint64()
+        _check(self.lib.dvm_remesh(self.h, p, n, C.byref(params), out, out_cap, C.byref(m)))
+        v = np.frombuffer(out, dtype=np.float64, count=4 * m.value).reshape(m.value, 4)
+        return tuple(v[:, k].copy() for k in range(4))
+
     def step_batch(self, sims, nsteps=1, use_graph=True):
         arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
         _check(self.lib.dvm_step_batch(self.h, arr, len(sims), nsteps, 1 if use_graph else 0))
@@ -422,6 +438,12 @@ class Simulation:
     def check(self):
         _check(self.lib.dvm_sim_status(self.h))
 
+    def remesh(self, params: "RemeshParams") -> int:
+        """Remesh in place on the device; returns the new blob count."""
+        n = C.c_uint64()
+        _check(self.lib.dvm_sim_remesh(self.h, C.byref(params), C.byref(n)))
+        return n.value
+
     def probe(self, px, pz):
         """Velocity at probe points: (u, w, uvs, wvs) with u, w the total."""
         px, pz = _f64(px), _f64(pz)
@@ -462,6 +484,22 @@ class ServerSummary(C.Structure):
                 ("retire_s", C.c_double), ("tunings", C.c_uint32)]
 
 
+REMESH_M4PRIME, REMESH_M6, REMESH_GAUSSIAN = 0, 1, 2
+
+
+class RemeshParams(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("zmin", C.c_double),
+                ("zmax", C.c_double), ("dx", C.c_double), ("dz", C.c_double),
+                ("sigma", C.c_double), ("circ_threshold", C.c_double), ("kernel", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+def remesh_grid(params: RemeshParams):
+    nx, nz = C.c_uint32(), C.c_uint32()
+    _check(load().dvm_remesh_grid(C.byref(params), C.byref(nx), C.byref(nz)))
+    return nx.value, nz.value
+
+
 class PairConfig(C.Structure):
     _fields_ = [("tile", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32),
                 ("reserved", C.c_int32)]
@@ -500,6 +538,11 @@ SIGNATURES.update({
                                        C.POINTER(PairConfig), C.POINTER(C.c_int)]),
     "dvm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]),
     "dvm_sim_probe": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]),
+    "dvm_remesh_grid": (C.c_int, [C.POINTER(RemeshParams), C.POINTER(C.c_uint32),
+                                  C.POINTER(C.c_uint32)]),
+    "dvm_sim_remesh": (C.c_int, [C.c_void_p, C.POINTER(RemeshParams), C.POINTER(C.c_uint64)]),
+    "dvm_remesh": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(RemeshParams),
+                             C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
 })
 
 

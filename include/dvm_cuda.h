@@ -241,6 +241,36 @@ int dvm_sim_status(dvm_sim* sim);
 int dvm_sim_clear_status(dvm_sim* sim);
 int dvm_sim_phase(dvm_sim* sim, int phase);
 int dvm_sim_step(dvm_sim* sim, int nsteps);
+/* Remeshing (BackgroundMesh; src/DVMBase.cpp:91-92, 160-164, options
+ * src/XmlHandler.cpp:191-201 -- its source is not part of the reference, the
+ * behaviour follows tests/unit/test_BackgroundMesh.cpp).  Nodes x = xmin + i dx
+ * (i <= (xmax - xmin) / dx), z likewise.  Every blob whose kernel support lies
+ * inside the mesh spreads its circulation to the nodes with the tensor-product
+ * weight W(xi - i) W(zeta - j) (node units; M4' support 2, M6 support 3,
+ * Gaussian truncated at 3 and normalised per blob); nodes with |circulation| >
+ * circ_threshold become the new blobs (core size sigma, row-major), followed by
+ * the blobs whose support leaves the mesh, unchanged.  IDs are renumbered and
+ * velocities zeroed.  Deterministic (no atomics). */
+#define DVM_REMESH_M4PRIME 0
+#define DVM_REMESH_M6 1
+#define DVM_REMESH_GAUSSIAN 2
+typedef struct {
+    double xmin, xmax, zmin, zmax; /* remesh/xmin ... remesh/zmax */
+    double dx, dz;                 /* remesh/dx, remesh/dz */
+    double sigma;                  /* remesh/sigma: core size of the new blobs */
+    double circ_threshold;         /* remesh/circ_threshold */
+    int32_t kernel;                /* DVM_REMESH_* (remesh/kernel) */
+    int32_t reserved;
+} dvm_remesh_params;
+/* Node counts of the mesh the parameters describe (at most 2^28 nodes). */
+int dvm_remesh_grid(const dvm_remesh_params* p, uint32_t* nx, uint32_t* nz);
+/* Remesh a simulation in place on the device; DVM_ERR_CAPACITY (state left
+ * unchanged) when the new blob set exceeds its capacity.  n_out may be null. */
+int dvm_sim_remesh(dvm_sim* sim, const dvm_remesh_params* p, uint64_t* n_out);
+/* The same on host arrays (BackgroundMesh::remesh(VortexBlobs)): *n_out = the
+ * new count; DVM_ERR_CAPACITY when it exceeds out_cap (out untouched). */
+int dvm_remesh(dvm_ctx* ctx, const dvm_particle* in, uint64_t n, const dvm_remesh_params* p,
+               dvm_particle* out, uint64_t out_cap, uint64_t* n_out);
 /* Velocity at probe points (host arrays, n of them) from the simulation's
  * current blobs, sheet and free stream: the intended formula of
  * VortexSheet::probe_velocities (src/VortexSheet.cpp:559-646), i.e. what a

@@ -647,3 +647,107 @@ void or_sim_get_forces(const or_sim* s, double* fx, double* fz, double* area) {
 }
 
 const double* or_sim_infm(const or_sim* s) { return s->A; }
+
+
+/* ---- remeshing (restated from the test formulas; see the header) ------------------ */
+static double rm_w(int kernel, double r) {
+    r = fabs(r);
+    if (kernel == 0) {
+        if (r < 1.0) return 1.0 - 2.5 * (r * r) + 1.5 * ((r * r) * r);
+        if (r < 2.0) {
+            const double t = 2.0 - r;
+            return ((0.5 * t) * t) * (1.0 - r);
+        }
+        return 0.0;
+    }
+    if (!(r < 3.0)) return 0.0;
+    if (kernel == 1) {
+        double a = 3.0 - r, b = 2.0 - r, c = 1.0 - r;
+        a = a > 0.0 ? ((a * a) * (a * a)) * a : 0.0;
+        b = b > 0.0 ? ((b * b) * (b * b)) * b : 0.0;
+        c = c > 0.0 ? ((c * c) * (c * c)) * c : 0.0;
+        return ((a - 6.0 * b) + 15.0 * c) / 120.0;
+    }
+    return exp(-0.5 * (r * r)) * 0.398942280401432677939946;
+}
+
+size_t or_remesh(const double* x, const double* z, const double* circ, const double* sigma,
+                 size_t n, double x0, double z0, double dx, double dz, int nx, int nz, int kernel,
+                 double new_sigma, double threshold, double* ox, double* oz, double* oc,
+                 double* os, size_t cap) {
+    const int S = kernel == 0 ? 2 : 3;
+    const size_t nn = (size_t)nx * (size_t)nz;
+    long long* cell = (long long*)malloc(sizeof(long long) * (n ? n : 1));
+    double* g = (double*)malloc(sizeof(double) * (n ? n : 1));
+    size_t* cstart = (size_t*)calloc(nn + 1, sizeof(size_t));
+    size_t* order = (size_t*)malloc(sizeof(size_t) * (n ? n : 1));
+    double* node = (double*)malloc(sizeof(double) * nn);
+    for (size_t p = 0; p < n; ++p) {
+        const double xi = (x[p] - x0) / dx, ze = (z[p] - z0) / dz;
+        cell[p] = -1;
+        g[p] = circ[p];
+        if (!(fabs(xi) < 1e9) || !(fabs(ze) < 1e9)) continue;
+        const long long fx = (long long)floor(xi), fz = (long long)floor(ze);
+        if (fx - (S - 1) < 0 || fx + S > nx - 1 || fz - (S - 1) < 0 || fz + S > nz - 1) continue;
+        cell[p] = fz * nx + fx;
+        if (kernel == 2) {
+            double sx = 0.0, sz = 0.0;
+            for (long long i = fx - (S - 1); i <= fx + S; ++i) sx = sx + rm_w(2, xi - (double)i);
+            for (long long j = fz - (S - 1); j <= fz + S; ++j) sz = sz + rm_w(2, ze - (double)j);
+            g[p] = g[p] / (sx * sz);
+        }
+    }
+    /* stable bucketing by cell (counting sort) */
+    for (size_t p = 0; p < n; ++p)
+        if (cell[p] >= 0) cstart[cell[p] + 1]++;
+    for (size_t c = 0; c < nn; ++c) cstart[c + 1] += cstart[c];
+    {
+        size_t* fill = (size_t*)malloc(sizeof(size_t) * (nn ? nn : 1));
+        memcpy(fill, cstart, sizeof(size_t) * nn);
+        for (size_t p = 0; p < n; ++p)
+            if (cell[p] >= 0) order[fill[cell[p]]++] = p;
+        free(fill);
+    }
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < (long long)nn; ++k) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        double acc = 0.0;
+        for (int b = j - S < 0 ? 0 : j - S; b <= (j + S - 1 < nz - 1 ? j + S - 1 : nz - 1); ++b)
+            for (int a = i - S < 0 ? 0 : i - S; a <= (i + S - 1 < nx - 1 ? i + S - 1 : nx - 1); ++a) {
+                const size_t c = (size_t)b * nx + a;
+                for (size_t q = cstart[c]; q < cstart[c + 1]; ++q) {
+                    const size_t p = order[q];
+                    const double xi = (x[p] - x0) / dx, ze = (z[p] - z0) / dz;
+                    acc = acc + (rm_w(kernel, xi - (double)i) * rm_w(kernel, ze - (double)j)) * g[p];
+                }
+            }
+        node[k] = acc;
+    }
+    size_t o = 0;
+    for (size_t k = 0; k < nn; ++k)
+        if (fabs(node[k]) > threshold) {
+            if (o < cap) {
+                ox[o] = x0 + (double)(k % nx) * dx;
+                oz[o] = z0 + (double)(k / nx) * dz;
+                oc[o] = node[k];
+                os[o] = new_sigma;
+            }
+            ++o;
+        }
+    for (size_t p = 0; p < n; ++p)
+        if (cell[p] < 0) {
+            if (o < cap) {
+                ox[o] = x[p];
+                oz[o] = z[p];
+                oc[o] = circ[p];
+                os[o] = sigma[p];
+            }
+            ++o;
+        }
+    free(cell);
+    free(g);
+    free(cstart);
+    free(order);
+    free(node);
+    return o;
+}

@@ -57,6 +57,18 @@ void or_release_place(const double* xp, const double* zp, const double* ds, cons
                       double* sigma);
 /* src/VortexSheet.cpp:447-464 — crossing number == 1. */
 int or_inside(const double* xp, const double* zp, int np, double x, double z);
+/* Remeshing (BackgroundMesh: source absent from the reference; behaviour from
+ * tests/unit/test_BackgroundMesh.cpp and options src/XmlHandler.cpp:191-201).
+ * kernel 0 M4', 1 M6, 2 Gaussian truncated at 3 (normalised per blob).  Nodes
+ * x0 + i dx, i < nx; z likewise.  Each node sums, in a fixed order (cells
+ * around it row-major, blobs in index order within a cell), W(xi-i) W(ze-j)
+ * circ of the blobs whose support lies inside the mesh; nodes with |sum| >
+ * threshold become blobs (row-major), then the other blobs follow unchanged.
+ * Writes at most cap blobs; returns the total count. */
+size_t or_remesh(const double* x, const double* z, const double* circ, const double* sigma,
+                 size_t n, double x0, double z0, double dx, double dz, int nx, int nz, int kernel,
+                 double new_sigma, double threshold, double* ox, double* oz, double* oc,
+                 double* os, size_t cap);
 /* src/VortexSheet.cpp:345-405 — reflect inside blobs; returns how many moved. */
 size_t or_reflect(const double* xp, const double* zp, const double* enx, const double* enz, int np,
                   double* x, double* z, size_t n);

@@ -219,6 +219,18 @@ class Port:
                           rho, dt, Ur, C.byref(fx), C.byref(fz))
         return fx.value, fz.value
 
+    def remesh(self, x, z, circ, sigma, x0, z0, dx, dz, nx, nz, kernel, new_sigma, threshold):
+        x, z, circ, sigma = map(_f64, (x, z, circ, sigma))
+        cap = nx * nz + x.size
+        out = [np.empty(max(cap, 1)) for _ in range(4)]
+        f = self.lib.or_remesh
+        f.restype = C.c_size_t
+        m = f(_ptr(x), _ptr(z), _ptr(circ), _ptr(sigma), C.c_size_t(x.size), C.c_double(x0),
+              C.c_double(z0), C.c_double(dx), C.c_double(dz), C.c_int(nx), C.c_int(nz),
+              C.c_int(kernel), C.c_double(new_sigma), C.c_double(threshold),
+              *[_ptr(a) for a in out], C.c_size_t(cap))
+        return [a[:m].copy() for a in out]
+
     def mt_stream(self, seed, n):
         out = np.empty(n)
         self.lib.or_mt_stream(seed, n, _ptr(out))
