@@ -23,7 +23,8 @@ BUILD_DIR = os.path.join(HERE, "_build")
 CUDA_SO = os.path.join(LIB_DIR, "libdvm_cuda.so")
 HOST_SO = os.path.join(LIB_DIR, "libdvmpp_host.so")
 
-CU_SOURCES = ["k_biot_savart.cu", "k_sheet.cu", "k_book.cu", "k_remesh.cu", "dvm_capi.cu",
+CU_SOURCES = ["k_biot_savart.cu", "k_sheet.cu", "k_book.cu", "k_remesh.cu", "k_merge.cu",
+              "dvm_capi.cu",
               "dvm_serve.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

@@ -1682,6 +1682,76 @@ int dvm_biot_savart_at_device(dvm_ctx* c, const double* x, const double* z, cons
     return DVM_OK;
 }
 
+// ---- vortex merging ----------------------------------------------------------------------
+int dvm_sim_merge(dvm_sim* s, double threshold, uint64_t* merged) {
+    if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    dvm_ctx* c = s->ctx;
+    uint32_t cnt = 0;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        CK(cudaSetDevice(c->device));
+        uint32_t n = 0;
+        CK(cudaMemcpyAsync(&n, &c->d_state[s->slot].n, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        void* scratch = nullptr;
+        const cudaError_t e = pool_alloc(c, &scratch, merge_scratch_bytes(n));
+        if (e != cudaSuccess)
+            return fail(DVM_ERR_OOM, std::string("merge scratch: ") + cudaGetErrorString(e));
+        const InstDesc& h = s->h;
+        uint32_t* cdev =
+            reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + merge_count_offset(n));
+        merge_run(MergeArrays{h.x, h.z, h.circ, h.sigma, h.u, h.w, h.uvs, h.wvs}, h.id, n,
+                  threshold, &c->d_state[s->slot].n, cdev, scratch, c->sms, c->stream);
+        CK(cudaMemcpyAsync(&cnt, cdev, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        pool_free(c, scratch);
+        g_launches += 4;
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    if (merged) *merged = cnt;
+    return DVM_OK;
+}
+
+int dvm_merge_blobs(dvm_ctx* c, double* x, double* z, double* circ, double* sigma, double* u,
+                    double* w, double* uvs, double* wvs, uint32_t* id, uint64_t n,
+                    double threshold, uint64_t* n_out, uint64_t* merged) {
+    if (!c || !n_out || (n && (!x || !z || !circ || !sigma || !u || !w || !uvs || !wvs)))
+        return fail(DVM_ERR_ARG, "null argument");
+    if (n > 0xF0000000ull) return fail(DVM_ERR_ARG, "too many blobs");
+    *n_out = n;
+    if (merged) *merged = 0;
+    if (n < 2) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    int rc = raw_reserve(c, 8 * 8 * (size_t)n);
+    if (rc) return rc;
+    double* d = static_cast<double*>(c->raw_block);
+    double* const host[8] = {x, z, circ, sigma, u, w, uvs, wvs};
+    for (int k = 0; k < 8; ++k)
+        CK(cudaMemcpyAsync(d + k * n, host[k], 8 * n, cudaMemcpyHostToDevice, c->stream));
+    void* scratch = nullptr;
+    const uint32_t nn = (uint32_t)n;
+    const cudaError_t e = pool_alloc(c, &scratch, merge_scratch_bytes(nn));
+    if (e != cudaSuccess) return fail(DVM_ERR_OOM, std::string("merge scratch: ") + cudaGetErrorString(e));
+    uint32_t* cdev = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + merge_count_offset(nn));
+    merge_run(MergeArrays{d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, d + 5 * n, d + 6 * n, d + 7 * n},
+              nullptr, nn, threshold, nullptr, cdev, scratch, c->sms, c->stream);
+    uint32_t cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, cdev, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    pool_free(c, scratch);
+    g_launches += 4;
+    CK(cudaStreamSynchronize(c->stream));
+    const uint64_t m = n - cnt;
+    for (int k = 0; k < 8; ++k)
+        CK(cudaMemcpyAsync(host[k], d + k * n, 8 * m, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (cnt && id)
+        for (uint64_t q = 0; q < m; ++q) id[q] = (uint32_t)q;
+    *n_out = m;
+    if (merged) *merged = cnt;
+    return DVM_OK;
+}
+
 // ---- remeshing -------------------------------------------------------------------------
 static int remesh_grid_of(const dvm_remesh_params* p, RemeshGrid* g) {
     if (!p) return fail(DVM_ERR_ARG, "remesh parameters are null");

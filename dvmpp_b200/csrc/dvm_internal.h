@@ -205,6 +205,16 @@ void remesh_run(const RemeshGrid& g, const double* x, const double* z, const dou
                 const double* sigma, uint32_t n, uint32_t cap, const RemeshDest& dest,
                 int* status, void* scratch, int sms, cudaStream_t s);
 
+// Vortex merging (k_merge.cu), in place on 8 SoA arrays of n blobs; the merge
+// count goes to scratch + merge_count_offset(n), the new length to n_dev.
+struct MergeArrays {
+    double *x, *z, *circ, *sigma, *u, *w, *uvs, *wvs;
+};
+size_t merge_scratch_bytes(uint32_t n);
+size_t merge_count_offset(uint32_t n);
+void merge_run(const MergeArrays& a, uint32_t* id, uint32_t n, double threshold,
+               uint32_t* n_dev, uint32_t* count_dev, void* scratch, int sms, cudaStream_t s);
+
 // Sheet velocity at arbitrary points from one simulation's panels and gamma
 // (the sheet-on-blob sum of src/VortexSheet.cpp:217-273, FP64), for probes.
 void sheet_at(const InstDesc& d, const double* px, const double* pz, uint32_t n, double* uvs,

@@ -31,9 +31,14 @@ DVMBase::DVMBase(XmlHandler& xml, const std::string& stamp)
         m_rng_mode = xml.getStringAttribute("algorithms", "diffusion_rng") == "philox"
                          ? DVM_RNG_PHILOX
                          : DVM_RNG_INJECT;
-    if (xml.has("algorithms", "merge_frequency") && xml.getValueAttribute("algorithms", "merge_frequency") > 0)
-        std::cout << "Vortex merging is not part of this build; merge options are ignored"
-                  << std::endl;
+    // src/DVMBase.cpp:51-64
+    if (xml.has("algorithms", "merge_threshold") && xml.has("algorithms", "merge_frequency")) {
+        m_merge_threshold = xml.getValueAttribute("algorithms", "merge_threshold");
+        m_merge_frequency = static_cast<unsigned>(xml.getIntAttribute("algorithms", "merge_frequency"));
+    }
+    if (m_merge_frequency > 0 && m_merge_threshold > 0)
+        std::cout << "Vortex merging enabled: threshold = " << m_merge_threshold
+                  << ", frequency = " << m_merge_frequency << std::endl;
     if (m_mesh.is_enabled())  // as src/DVMBase.cpp:61-64 reports merging
         std::cout << "Remeshing enabled: " << m_mesh.nx() << " x " << m_mesh.nz()
                   << " mesh nodes" << std::endl;
@@ -115,6 +120,12 @@ void DVMBase::compute_step() {
             dvm::check_status(dvm_sim_phase(m_sim, ph), "DVMBase::compute_step");
     }
     dvm::check_status(dvm_sim_status(m_sim), "DVMBase::compute_step");
+    // merge after the loads (src/DVMBase.cpp:124-132), on the device
+    if (m_merge_frequency > 0 && m_merge_threshold > 0 && m_step % m_merge_frequency == 0) {
+        uint64_t merged = 0;
+        dvm::check_status(dvm_sim_merge(m_sim, m_merge_threshold, &merged), "DVMBase merge");
+        if (merged > 0) std::cout << "Merged " << merged << " vortex pairs" << std::endl;
+    }
 }
 
 void DVMBase::convect() { dvm::check_status(dvm_sim_phase(m_sim, DVM_PHASE_CONVECT), "convect"); }

@@ -36,6 +36,8 @@ class DVMBase
     BackgroundMesh m_mesh;
     double m_nu = 0, m_Ux = 0, m_Uz = 0, m_Ur = 0, m_dt = 0, m_time = 0;
     unsigned m_step = 0, m_steps = 0;
+    double m_merge_threshold = 0.0;  // algorithms/merge_threshold
+    unsigned m_merge_frequency = 0;  // algorithms/merge_frequency
     Scheme m_scheme = Scheme::Euler;
     SurfaceCross m_surfcross = SurfaceCross::Reflect;
     int m_rng_mode = DVM_RNG_INJECT;

@@ -87,10 +87,28 @@ void VortexBlobs::copyOutputConfig(const VortexBlobs& o) {
     m_numfile = o.m_numfile;
 }
 
-unsigned VortexBlobs::merge_blobs(double) {
-    throw dvm::AlgorithmException(
-        "VortexBlobs::merge_blobs is not part of the B200 build (vortex merging is off by "
-        "default in the reference and outside the accelerated path)");
+unsigned VortexBlobs::merge_blobs(double threshold) {
+    // src/VortexBlobs.cpp:110-209 on the GPU (dvm_merge_blobs): the same greedy
+    // order and arithmetic, so the same merged set, bit for bit
+    const uint64_t n = size();
+    if (n < 2) return 0;
+    Vector* const arr[8] = {&m_x, &m_z, &m_circ, &m_sigma, &m_u, &m_w, &m_uvs, &m_wvs};
+    std::vector<std::vector<double>> v(8);
+    for (int k = 0; k < 8; ++k) v[k].assign(arr[k]->memptr(), arr[k]->memptr() + n);
+    std::vector<uint32_t> ids(n);
+    for (uint64_t i = 0; i < n; ++i) ids[i] = m_ID[i];
+    uint64_t m = n, merged = 0;
+    dvm::check_status(dvm_merge_blobs(dvm::device_context(), v[0].data(), v[1].data(),
+                                      v[2].data(), v[3].data(), v[4].data(), v[5].data(),
+                                      v[6].data(), v[7].data(), ids.data(), n, threshold, &m,
+                                      &merged),
+                      "VortexBlobs::merge_blobs");
+    if (merged == 0) return 0;
+    resize((unsigned)m);
+    for (int k = 0; k < 8; ++k)
+        for (uint64_t i = 0; i < m; ++i) (*arr[k])(i) = v[k][i];
+    for (uint64_t i = 0; i < m; ++i) m_ID[i] = ids[i];
+    return (unsigned)merged;
 }
 
 void VortexBlobs::append_vortices(VortexBlobs& nb) {

@@ -227,6 +227,21 @@ class Context:
         v = np.frombuffer(out, dtype=np.float64, count=2 * nt).reshape(nt, 2) if nt else np.zeros((0, 2))
         return v[:, 0].copy(), v[:, 1].copy()
 
+    def merge_blobs(self, d: dict, threshold: float):
+        """Greedy merge on host arrays (the VortexBlobs::merge_blobs path).
+        d: x z circ sigma u w uvs wvs (+ id); returns (new dict, merge count)."""
+        keys = ["x", "z", "circ", "sigma", "u", "w", "uvs", "wvs"]
+        arrs = [np.array(d[k], dtype=np.float64) for k in keys]
+        n = arrs[0].size
+        ids = np.array(d.get("id", np.arange(n)), dtype=np.uint32)
+        m, cnt = C.c_uint64(), C.c_uint64()
+        _check(self.lib.dvm_merge_blobs(self.h, *[_p(a) for a in arrs],
+                                        ids.ctypes.data_as(_u32p), n, threshold, C.byref(m),
+                                        C.byref(cnt)))
+        out = {k: a[:m.value].copy() for k, a in zip(keys, arrs)}
+        out["id"] = ids[:m.value].copy()
+        return out, cnt.value
+
     def remesh(self, x, z, circ, sigma, params: RemeshParams, out_cap=None):
         """Remesh host arrays (the BackgroundMesh::remesh path): (x, z, circ, sigma)."""
         n = len(x)
@@ -438,6 +453,12 @@ class Simulation:
     def check(self):
         _check(self.lib.dvm_sim_status(self.h))
 
+    def merge(self, threshold: float) -> int:
+        """Greedy vortex merge in place on the device; returns the merge count."""
+        m = C.c_uint64()
+        _check(self.lib.dvm_sim_merge(self.h, threshold, C.byref(m)))
+        return m.value
+
     def remesh(self, params: "RemeshParams") -> int:
         """Remesh in place on the device; returns the new blob count."""
         n = C.c_uint64()
@@ -538,6 +559,10 @@ SIGNATURES.update({
                                        C.POINTER(PairConfig), C.POINTER(C.c_int)]),
     "dvm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]),
     "dvm_sim_probe": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]),
+    "dvm_sim_merge": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_uint64)]),
+    "dvm_merge_blobs": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _u32p,
+                                  C.c_uint64, C.c_double, C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint64)]),
     "dvm_remesh_grid": (C.c_int, [C.POINTER(RemeshParams), C.POINTER(C.c_uint32),
                                   C.POINTER(C.c_uint32)]),
     "dvm_sim_remesh": (C.c_int, [C.c_void_p, C.POINTER(RemeshParams), C.POINTER(C.c_uint64)]),

@@ -241,6 +241,17 @@ int dvm_sim_status(dvm_sim* sim);
 int dvm_sim_clear_status(dvm_sim* sim);
 int dvm_sim_phase(dvm_sim* sim, int phase);
 int dvm_sim_step(dvm_sim* sim, int nsteps);
+/* Vortex merging, VortexBlobs::merge_blobs (src/VortexBlobs.cpp:110-209): the
+ * reference's greedy merge in index order (each surviving blob absorbs every
+ * later unmerged blob with |gi gj / (gi + gj)| |xi - xj| < threshold, its state
+ * updated after each absorption), then merged blobs removed and IDs renumbered
+ * (unchanged when nothing merged).  Bit-identical to the reference.  In place on
+ * the device (dvm_sim_merge) or on host arrays of n blobs (dvm_merge_blobs; id
+ * may be null); *merged = the merge count. */
+int dvm_sim_merge(dvm_sim* sim, double threshold, uint64_t* merged);
+int dvm_merge_blobs(dvm_ctx* ctx, double* x, double* z, double* circ, double* sigma, double* u,
+                    double* w, double* uvs, double* wvs, uint32_t* id, uint64_t n,
+                    double threshold, uint64_t* n_out, uint64_t* merged);
 /* Remeshing (BackgroundMesh; src/DVMBase.cpp:91-92, 160-164, options
  * src/XmlHandler.cpp:191-201 -- its source is not part of the reference, the
  * behaviour follows tests/unit/test_BackgroundMesh.cpp).  Nodes x = xmin + i dx

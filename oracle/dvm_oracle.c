@@ -751,3 +751,52 @@ size_t or_remesh(const double* x, const double* z, const double* circ, const dou
     free(node);
     return o;
 }
+
+
+/* ---- vortex merging, src/VortexBlobs.cpp:110-209 ----------------------------------- */
+unsigned or_merge_blobs(double* x, double* z, double* circ, double* sigma, double* u, double* w,
+                        double* uvs, double* wvs, unsigned* id, size_t n, double threshold,
+                        size_t* n_out) {
+    *n_out = n;
+    if (n < 2) return 0;
+    unsigned char* merged = (unsigned char*)calloc(n, 1);
+    unsigned count = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (merged[i]) continue;
+        for (size_t j = i + 1; j < n; ++j) {
+            if (merged[j]) continue;
+            const double gi = circ[i], gj = circ[j];
+            const double gs = gi + gj;
+            if (fabs(gs) < 1e-15) continue;
+            const double dx = x[i] - x[j], dz = z[i] - z[j];
+            const double dist = sqrt(dx * dx + dz * dz);
+            const double crit = fabs(gi * gj / gs) * dist;
+            if (crit < threshold) {
+                const double nx_ = (gi * x[i] + gj * x[j]) / gs;
+                const double nz_ = (gi * z[i] + gj * z[j]) / gs;
+                const double ns = (fabs(gi) * sigma[i] + fabs(gj) * sigma[j]) / (fabs(gi) + fabs(gj));
+                x[i] = nx_;
+                z[i] = nz_;
+                circ[i] = gs;
+                sigma[i] = ns;
+                u[i] = w[i] = uvs[i] = wvs[i] = 0.0;
+                merged[j] = 1;
+                ++count;
+            }
+        }
+    }
+    size_t o = 0;
+    if (count)
+        for (size_t i = 0; i < n; ++i) {
+            if (merged[i]) continue;
+            x[o] = x[i]; z[o] = z[i]; circ[o] = circ[i]; sigma[o] = sigma[i];
+            u[o] = u[i]; w[o] = w[i]; uvs[o] = uvs[i]; wvs[o] = wvs[i];
+            id[o] = (unsigned)o;
+            ++o;
+        }
+    else
+        o = n;
+    free(merged);
+    *n_out = o;
+    return count;
+}

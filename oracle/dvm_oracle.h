@@ -57,6 +57,14 @@ void or_release_place(const double* xp, const double* zp, const double* ds, cons
                       double* sigma);
 /* src/VortexSheet.cpp:447-464 — crossing number == 1. */
 int or_inside(const double* xp, const double* zp, int np, double x, double z);
+/* src/VortexBlobs.cpp:110-209 — greedy pairwise merge in index order (each
+ * surviving i absorbs, one after another, every later unmerged j with
+ * |gi gj / (gi + gj)| |xi - xj| < threshold, using i's updated state), then a
+ * stable compaction with IDs renumbered.  In place on the 8 SoA arrays + ids;
+ * returns the merge count, the new length in *n_out. */
+unsigned or_merge_blobs(double* x, double* z, double* circ, double* sigma, double* u, double* w,
+                        double* uvs, double* wvs, unsigned* id, size_t n, double threshold,
+                        size_t* n_out);
 /* Remeshing (BackgroundMesh: source absent from the reference; behaviour from
  * tests/unit/test_BackgroundMesh.cpp and options src/XmlHandler.cpp:191-201).
  * kernel 0 M4', 1 M6, 2 Gaussian truncated at 3 (normalised per blob).  Nodes

@@ -231,6 +231,21 @@ class Port:
               *[_ptr(a) for a in out], C.c_size_t(cap))
         return [a[:m].copy() for a in out]
 
+    def merge_blobs(self, d, threshold):
+        """d: dict of x z circ sigma u w uvs wvs id; returns (new dict, merge count)."""
+        keys = ["x", "z", "circ", "sigma", "u", "w", "uvs", "wvs"]
+        arrs = [np.array(d[k], dtype=np.float64) for k in keys]
+        ids = np.array(d["id"], dtype=np.uint32)
+        n_out = C.c_size_t()
+        f = self.lib.or_merge_blobs
+        f.restype = C.c_uint
+        cnt = f(*[_ptr(a) for a in arrs], ids.ctypes.data_as(C.POINTER(C.c_uint)),
+                C.c_size_t(ids.size), C.c_double(threshold), C.byref(n_out))
+        m = n_out.value
+        out = {k: a[:m].copy() for k, a in zip(keys, arrs)}
+        out["id"] = ids[:m].copy()
+        return out, int(cnt)
+
     def mt_stream(self, seed, n):
         out = np.empty(n)
         self.lib.or_mt_stream(seed, n, _ptr(out))
@@ -387,6 +402,20 @@ class Ref:
                                   tx.size, _ptr(u), _ptr(w)):
             raise RuntimeError(self.err())
         return u, w
+
+    def merge_blobs(self, d, threshold):
+        keys = ["x", "z", "circ", "sigma", "u", "w", "uvs", "wvs"]
+        arrs = [np.array(d[k], dtype=np.float64) for k in keys]
+        ids = np.array(d["id"], dtype=np.uint32)
+        n_out, cnt = C.c_size_t(), C.c_uint()
+        if self.lib.ref_merge_blobs(*[_ptr(a) for a in arrs],
+                                    ids.ctypes.data_as(C.POINTER(C.c_uint)), C.c_size_t(ids.size),
+                                    C.c_double(threshold), C.byref(n_out), C.byref(cnt)):
+            raise RuntimeError(self.err())
+        m = n_out.value
+        out = {k: a[:m].copy() for k, a in zip(keys, arrs)}
+        out["id"] = ids[:m].copy()
+        return out, int(cnt.value)
 
     def random_stream(self, seed, n):
         out = np.empty(n)

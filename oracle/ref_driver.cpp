@@ -98,6 +98,34 @@ int ref_direct_at(const double* x, const double* z, const double* circ, const do
     }
 }
 
+// ---- VortexBlobs::merge_blobs (src/VortexBlobs.cpp:110-209) ---------------
+// In/out arrays of length n (8 SoA arrays + ids); returns the merge count, the
+// new length in *n_out.
+int ref_merge_blobs(double* x, double* z, double* circ, double* sigma, double* u, double* w,
+                    double* uvs, double* wvs, unsigned* id, size_t n, double threshold,
+                    size_t* n_out, unsigned* merged) {
+    try {
+        VortexBlobs b((unsigned)n);
+        for (size_t i = 0; i < n; ++i) {
+            b.m_ID[i] = id[i];
+            b.m_x(i) = x[i]; b.m_z(i) = z[i]; b.m_circ(i) = circ[i]; b.m_sigma(i) = sigma[i];
+            b.m_u(i) = u[i]; b.m_w(i) = w[i]; b.m_uvs(i) = uvs[i]; b.m_wvs(i) = wvs[i];
+        }
+        *merged = b.merge_blobs(threshold);
+        const size_t m = b.size();
+        for (size_t i = 0; i < m; ++i) {
+            id[i] = b.m_ID[i];
+            x[i] = b.m_x(i); z[i] = b.m_z(i); circ[i] = b.m_circ(i); sigma[i] = b.m_sigma(i);
+            u[i] = b.m_u(i); w[i] = b.m_w(i); uvs[i] = b.m_uvs(i); wvs[i] = b.m_wvs(i);
+        }
+        *n_out = m;
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 // ---- Random (src/Random.cpp) ------------------------------------------------
 void ref_random_stream(int seed, size_t n, double* out) {
     Random r;

@@ -61,3 +61,28 @@ def test_phases_bitwise_on_a_wake(port, ref):
         for key in ("x", "z", "u", "w", "uvs", "wvs", "circ", "sigma"):
             assert np.array_equal(a[key], b[key]), (phase, key)
         assert np.array_equal(rs.gamma(), ps.gamma()), phase
+
+
+def _merge_case(n, seed):
+    rng = np.random.default_rng(seed)
+    d = {"x": rng.uniform(0, 2, n), "z": rng.uniform(-1, 1, n),
+         "circ": rng.normal(0, 1e-3, n), "sigma": rng.uniform(0.02, 0.05, n)}
+    for k in ("u", "w", "uvs", "wvs"):
+        d[k] = rng.normal(0, 1, n)
+    d["id"] = np.arange(n, dtype=np.uint32)
+    d["circ"][5] = 0.0              # zero circulation: merges at any distance
+    d["circ"][6] = -d["circ"][7]    # a cancelling pair: skipped
+    d["x"][9], d["z"][9] = d["x"][8], d["z"][8]  # coincident blobs
+    return d
+
+
+@pytest.mark.parametrize("thr", [0.0, 1e-7, 1e-6, 1e-5])
+def test_merge_blobs_bitwise(port, ref, thr):
+    """VortexBlobs::merge_blobs (src/VortexBlobs.cpp:110-209): the oracle's
+    restatement against the reference build, all 8 arrays and the IDs."""
+    d = _merge_case(3000, 3)
+    a, ca = port.merge_blobs(d, thr)
+    b, cb = ref.merge_blobs(d, thr)
+    assert ca == cb
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
