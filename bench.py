@@ -440,32 +440,55 @@ def run_ours(args, dist):
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
-        hbuf = [pinned(max(2 * s.n_hint + 8 * s.np + 64, 1)) for s in sims]
+        # The user's loop, pipelined as an application would run it: launch
+        # step k, generate the next step's uniforms on the host while the GPU
+        # computes, read step k's blobs and loads back, push the uniforms.
+        # Uniforms are pushed for an upper bound of the next step's draws (the
+        # device consumes them in order; the surplus carries over).
+        M = 3
+        ub = [2 * (s.n_hint + 2 * (M + 1) * s.np) + 2 * (M + 1) * s.np + 64 for s in sims]
+        hbuf = [[pinned(u) for u in ub] for _ in range(2)]
         out_x = [pinned(s.n_hint) for s in sims]
         out_z = [pinned(s.n_hint) for s in sims]
         out_c = [pinned(s.n_hint) for s in sims]
+        nprev = [s.n for s in sims]
+
+        def generate(bufs):
+            sizes = []
+            for sm, hb, n in zip(sims, bufs, nprev):
+                need = 2 * (n + 2 * (M + 1) * sm.np) + 2 * (M + 1) * sm.np + 64
+                hb[:need] = 1.0 - rng.random(need)
+                sizes.append(need)
+            return sizes
+
         h2d = d2h = 0
         dist.barrier()
         ctx.sync()
         t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            for s, hb in zip(sims, hbuf):
-                n = s.n  # blob count before the step
-                need = 2 * n + 2 * (3 + 1) * s.np + 64
-                hb[:need] = 1.0 - rng.random(need)
-                s.push_uniforms(hb[:need])
-                h2d += need * 8
-            ctx.step_batch(sims, 1, use_graph=True)
-            for s, ox, oz, oc in zip(sims, out_x, out_z, out_c):
-                s.get_state_into(ox, oz, oc)
-                s.loads()
-                d2h += 3 * 8 * s.last_n + 4 * 8
+        sizes = generate(hbuf[0])
+        for sm, hb, k in zip(sims, hbuf[0], sizes):
+            sm.push_uniforms(hb[:k])
+            h2d += 8 * k
+        for step in range(args.e2e_steps):
+            ctx.step_batch(sims, 1, use_graph=True)  # asynchronous
+            last = step + 1 == args.e2e_steps
+            if not last:
+                sizes = generate(hbuf[(step + 1) % 2])  # overlaps the GPU step
+            for i, (sm, ox, oz, oc) in enumerate(zip(sims, out_x, out_z, out_c)):
+                nprev[i] = sm.get_state_into(ox, oz, oc)
+                sm.loads()
+                d2h += 3 * 8 * sm.last_n + 4 * 8
+            if not last:
+                for sm, hb, k in zip(sims, hbuf[(step + 1) % 2], sizes):
+                    sm.push_uniforms(hb[:k])
+                    h2d += 8 * k
         ctx.sync()
         e2e_s = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.world * args.instances * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d / args.e2e_steps),
                "d2h_bytes_per_step": int(d2h / args.e2e_steps),
-               "note": "per step: uniforms pushed (inject mode) from pinned host memory, one "
+               "note": "per step: the next step's uniforms (inject mode) generated on the "
+                       "host while the GPU computes and pushed from pinned memory, one "
                        "batched step, x/z/circ of every blob and the loads read back "
                        "(what DVMBase::write_outputs consumes); host wall clock"}
         for s in sims:
