@@ -6,17 +6,18 @@
 //               u_i = -(1/2pi) sum_j K dz Gamma_j,  w_i = (1/2pi) sum_j K dx Gamma_j
 //
 // FP32 path (the throughput path): blobs of every listed simulation are sorted
-// along a Morton curve, packed as (x, z, Gamma, sigma) in FP64 and split into
-// 256-blob tiles with bounding boxes.  A work item is (simulation, 1024 sorted
-// targets, one source chunk); the persistent grid pulls items from an atomic
-// counter.  Each warp owns 128 consecutive sorted targets, so it covers a
-// small region: for every staged source tile it checks, once, whether any of
-// its pairs can fall inside the 10 sigma^2 core.  Far tiles (almost all of
-// them) run the 8-instruction pair loop with no test; near tiles run the exact
-// test, expm1 for the core and the self-pair exclusion.  Coordinates are FP32
-// offsets from the item's first target (which keeps close pairs accurate),
-// sums are plain FP32 within a 256-source stage and Kahan-compensated across
-// stages; chunk partials are combined in FP64 in chunk order (deterministic).
+// along a Morton curve, packed as FP64 (x, z) + FP32 (Gamma, 10 sigma^2,
+// 1/sigma^2) and split into 256-blob tiles with bounding boxes.  A work item is
+// (simulation, 256 or 128 sorted targets, one source chunk); every warp pulls
+// items from an atomic counter on its own and stages 256 sources at a time in
+// its slice of shared memory.  Per staged tile the warp checks once whether any
+// of its pairs can fall inside the 10 sigma^2 core: far tiles (almost all) run
+// packed FP32x2 arithmetic with one MUFU reciprocal per pair and no test; near
+// tiles run the exact test with expm1 and the r -> 0 core limit.  Coordinates
+// are FP32 offsets from the first target of the enclosing 256-target block,
+// sums are FP32 within a stage and Kahan-compensated across stages, and chunk
+// partials are combined in FP64 in chunk order: deterministic, and independent
+// of the batch a simulation runs in and of the launch shape.
 //
 // FP64 path (the parity path): same work decomposition in original blob order
 // and the reference's exact operation sequence (no FMA contraction).
@@ -522,7 +523,7 @@ __global__ void __launch_bounds__(kBsThreads, 1)
                     const double r2 = dadd(dmul(dx, dx), dmul(dz, dz));
                     double K;
                     if (r2 < s.w) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
-                    else K = ddiv(1.0, r2);
+                    else K = __drcp_rn(r2);  // correctly rounded: the same value as 1.0 / r2
                     uu[r] = dsub(uu[r], dmul(dmul(K, dz), s.z));
                     ww[r] = dadd(ww[r], dmul(dmul(K, dx), s.z));
                 }
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                     if (J.skip_close && !(r2 > 1e-15)) continue;
                     double K;
                     if (r2 < s_thr[jj]) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
-                    else K = ddiv(1.0, r2);
+                    else K = __drcp_rn(r2);  // correctly rounded: the same value as 1.0 / r2
                     uu = dsub(uu, dmul(dmul(K, dz), s_c[jj]));
                     ww = dadd(ww, dmul(dmul(K, dx), s_c[jj]));
                 }
