@@ -100,3 +100,22 @@ def test_steps_with_merging_match_oracle(ctx, port):
         assert np.max(np.abs(d["circ"] - e["circ"])) <= 1e-12 * np.max(np.abs(e["circ"])), k
     assert total > 0
     s.close()
+
+
+@pytest.mark.parametrize("n,thr", [(20000, 2e-6), (20000, 5e-5), (60000, 1e-6)])
+def test_merge_grid_search_bitwise(ctx, port, n, thr):
+    """Above 4096 blobs candidates come from a cell grid plus a short list of
+    the smallest circulations; the merged set must still be the oracle's, bit
+    for bit (wake-like positions, a few zero and non-finite circulations)."""
+    d = {k: v for k, v in zip(("x", "z", "circ", "sigma"), W.wake(n, 7, 0.08))}
+    rng = np.random.default_rng(n)
+    for k in ("u", "w", "uvs", "wvs"):
+        d[k] = np.zeros(n)
+    d["id"] = np.arange(n, dtype=np.uint32)
+    d["circ"][rng.integers(0, n, 40)] = 0.0
+    d["x"][rng.integers(0, n, 3)] = np.inf
+    got, cg = ctx.merge_blobs(d, thr)
+    ref, cr = port.merge_blobs(d, thr)
+    assert cg == cr and cg > 0
+    for k in KEYS + ("id",):
+        assert np.array_equal(got[k], ref[k], equal_nan=True), k
