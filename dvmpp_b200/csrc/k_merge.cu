@@ -24,6 +24,12 @@
 // (g_cut: the smallest |g| in the grid), falling back to the full scan when that
 // radius is large or undefined.  The minimum over the candidates is the same
 // first qualifying j as the full scan's, so the result is unchanged.
+//
+// Most blobs absorb nothing.  A blob's state is still its original one when its
+// turn comes, and its later candidates then are a subset of the original later
+// blobs with their original states, so a blob with no qualifying partner among
+// those can be skipped: all SMs find, in parallel, the blobs that have one, and
+// the sequential walk visits only them.
 #include <cfloat>
 #include <algorithm>
 #include <cmath>
@@ -67,11 +73,64 @@ __device__ __forceinline__ bool merge_test(double xi, double zi, double gi, doub
     return crit < thr;
 }
 
+// Cell range to search for absorber state (xi, zi, gi); false: scan everything.
+__device__ __forceinline__ bool cell_range(const MergeGrid& G, double xi, double zi, double gi,
+                                           double thr, long long& cx0, long long& cx1,
+                                           long long& cz0, long long& cz1) {
+    if (!G.enabled) return false;
+    const double R = thr * (1.0 / G.g_cut + 1.0 / fabs(gi)) * (1.0 + 1e-9);
+    if (!(R < kCellReach * G.h) || !(fabs(xi) < 1e300) || !(fabs(zi) < 1e300)) return false;
+    // cell coordinates clamped as doubles before the integer conversion
+    auto cell = [&](double v, int nc) {
+        return (long long)floor(fmin(fmax(v, -2.0), (double)nc + 1.0));
+    };
+    cx0 = max(0LL, cell((xi - R - G.x0) * G.inv_h, G.nxc) - 1);
+    cx1 = min((long long)G.nxc - 1, cell((xi + R - G.x0) * G.inv_h, G.nxc) + 1);
+    cz0 = max(0LL, cell((zi - R - G.z0) * G.inv_h, G.nzc) - 1);
+    cz1 = min((long long)G.nzc - 1, cell((zi + R - G.z0) * G.inv_h, G.nzc) + 1);
+    return true;
+}
+
+// Whether blob i, in its original state, has a qualifying later partner.
+__global__ void k_mg_absorbers(const double* __restrict__ x, const double* __restrict__ z,
+                               const double* __restrict__ circ, uint32_t n, double thr,
+                               MergeGrid G, uint32_t* __restrict__ flag) {
+    const uint32_t n_grid = G.enabled ? G.n_grid[0] : 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double xi = x[i], zi = z[i], gi = circ[i];
+        bool found = false;
+        long long cx0, cx1, cz0, cz1;
+        if (cell_range(G, xi, zi, gi, thr, cx0, cx1, cz0, cz1)) {
+            for (long long cz = cz0; cz <= cz1 && !found; ++cz)
+                for (long long cx = cx0; cx <= cx1 && !found; ++cx) {
+                    const uint64_t c = (uint64_t)cz * G.nxc + cx;
+                    for (uint32_t q = G.cstart[c]; q < G.cend[c]; ++q) {
+                        const uint32_t j = G.svals[q];
+                        if (j > i && merge_test(xi, zi, gi, x[j], z[j], circ[j], thr)) {
+                            found = true;
+                            break;
+                        }
+                    }
+                }
+            for (uint32_t q = n_grid; q < n && !found; ++q) {
+                const uint32_t j = G.svals[q];
+                found = j > i && merge_test(xi, zi, gi, x[j], z[j], circ[j], thr);
+            }
+        } else {
+            for (uint32_t j = i + 1; j < n && !found; ++j)
+                found = merge_test(xi, zi, gi, x[j], z[j], circ[j], thr);
+        }
+        flag[i] = found ? 1u : 0u;
+    }
+}
+
 __global__ void __launch_bounds__(kMergeThreads, 1)
     k_merge_greedy(double* __restrict__ x, double* __restrict__ z, double* __restrict__ circ,
                    double* __restrict__ sigma, double* __restrict__ u, double* __restrict__ w,
                    double* __restrict__ uvs, double* __restrict__ wvs, uint32_t n, double thr,
-                   MergeGrid G, uint32_t* __restrict__ keep, uint32_t* __restrict__ count) {
+                   MergeGrid G, const uint32_t* __restrict__ absorbers,
+                   const uint32_t* __restrict__ n_abs, uint32_t* __restrict__ keep,
+                   uint32_t* __restrict__ count) {
     using Reduce = cub::BlockReduce<uint32_t, kMergeThreads>;
     __shared__ typename Reduce::TempStorage red;
     __shared__ double si[4];  // x, z, circ, sigma of the current absorber
@@ -81,8 +140,10 @@ __global__ void __launch_bounds__(kMergeThreads, 1)
     const uint32_t n_grid = G.enabled ? G.n_grid[0] : 0;
     __syncthreads();
     uint32_t merges = 0;
-    for (uint32_t i = 0; i + 1 < n; ++i) {
-        if (!keep[i]) continue;  // every thread reads the same value
+    const uint32_t na = n_abs[0];
+    for (uint32_t t = 0; t < na; ++t) {
+        const uint32_t i = absorbers[t];  // ascending: the reference's order
+        if (!keep[i]) continue;           // every thread reads the same value
         if (tid == 0) {
             si[0] = x[i];
             si[1] = z[i];
@@ -95,23 +156,8 @@ __global__ void __launch_bounds__(kMergeThreads, 1)
             const double xi = si[0], zi = si[1], gi = si[2];
             uint32_t best = UINT32_MAX;
             // cell range of this pass (the same decision in every thread)
-            bool full = !G.enabled;
             long long cx0 = 0, cx1 = -1, cz0 = 0, cz1 = -1;
-            if (!full) {
-                const double R = thr * (1.0 / G.g_cut + 1.0 / fabs(gi)) * (1.0 + 1e-9);
-                if (!(R < kCellReach * G.h) || !(fabs(xi) < 1e300) || !(fabs(zi) < 1e300)) {
-                    full = true;
-                } else {
-                    // cell coordinates clamped as doubles before the integer conversion
-                    auto cell = [&](double v, int nc) {
-                        return (long long)floor(fmin(fmax(v, -2.0), (double)nc + 1.0));
-                    };
-                    cx0 = max(0LL, cell((xi - R - G.x0) * G.inv_h, G.nxc) - 1);
-                    cx1 = min((long long)G.nxc - 1, cell((xi + R - G.x0) * G.inv_h, G.nxc) + 1);
-                    cz0 = max(0LL, cell((zi - R - G.z0) * G.inv_h, G.nzc) - 1);
-                    cz1 = min((long long)G.nzc - 1, cell((zi + R - G.z0) * G.inv_h, G.nzc) + 1);
-                }
-            }
+            const bool full = !cell_range(G, xi, zi, gi, thr, cx0, cx1, cz0, cz1);
             if (full) {
                 for (uint32_t j = j0 + tid; j < n; j += kMergeThreads) {
                     if (!keep[j]) continue;
@@ -263,7 +309,7 @@ __global__ void k_merge_copyback(const uint32_t* __restrict__ count, uint32_t n,
 
 struct MLayout {
     size_t keep, pos, tmp, tmp_bytes, t, count, gbits, gsorted, keys, skeys, vals, svals, cstart,
-        cend, part, scal, bytes;
+        cend, part, scal, aflag, alist, bytes;
 };
 
 constexpr int kStatBlocks = 256;
@@ -276,13 +322,16 @@ int sort_bits(uint64_t v) {
 
 MLayout mlayout(uint32_t n) {
     const uint64_t ncells = (uint64_t)kGridMax * kGridMax;
-    size_t scan_b = 0, sk_b = 0, sp_b = 0;
+    size_t scan_b = 0, sk_b = 0, sp_b = 0, sel_b = 0;
     const int64_t nn = (int64_t)std::max<uint32_t>(n, 1);
     cub::DeviceScan::ExclusiveSum(nullptr, scan_b, (const uint32_t*)nullptr, (uint32_t*)nullptr, nn);
     cub::DeviceRadixSort::SortKeys(nullptr, sk_b, (const uint64_t*)nullptr, (uint64_t*)nullptr, nn);
     cub::DeviceRadixSort::SortPairs(nullptr, sp_b, (const uint64_t*)nullptr, (uint64_t*)nullptr,
                                     (const uint32_t*)nullptr, (uint32_t*)nullptr, nn, 0,
                                     sort_bits(ncells));
+    cub::DeviceSelect::Flagged(nullptr, sel_b, cub::CountingInputIterator<uint32_t>(0),
+                               (const uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                               nn);
     MLayout L{};
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -292,7 +341,7 @@ MLayout mlayout(uint32_t n) {
     };
     L.keep = take(4ull * n + 4);
     L.pos = take(4ull * n + 4);
-    L.tmp_bytes = std::max({scan_b, sk_b, sp_b}) + 256;
+    L.tmp_bytes = std::max({scan_b, sk_b, sp_b, sel_b}) + 256;
     L.tmp = take(L.tmp_bytes);
     L.t = take(8 * 8ull * n + 8);
     L.count = take(64);
@@ -306,6 +355,8 @@ MLayout mlayout(uint32_t n) {
     L.cend = take(4 * ncells);
     L.part = take(sizeof(double4) * kStatBlocks);
     L.scal = take(64);
+    L.aflag = take(4ull * n + 4);
+    L.alist = take(4ull * n + 4);
     L.bytes = off;
     return L;
 }
@@ -398,8 +449,15 @@ void merge_run(const MergeArrays& a, uint32_t* id, uint32_t n, double threshold,
         return;
     }
     const MergeGrid G = build_grid(a, n, threshold, L, b, s);
+    uint32_t* aflag = reinterpret_cast<uint32_t*>(b + L.aflag);
+    uint32_t* alist = reinterpret_cast<uint32_t*>(b + L.alist);
+    uint32_t* n_abs = reinterpret_cast<uint32_t*>(b + L.scal) + 4;
+    k_mg_absorbers<<<sms * 4, 256, 0, s>>>(a.x, a.z, a.circ, n, threshold, G, aflag);
+    size_t sb = L.tmp_bytes;
+    cub::DeviceSelect::Flagged(b + L.tmp, sb, cub::CountingInputIterator<uint32_t>(0), aflag,
+                               alist, n_abs, (int64_t)n, s);
     k_merge_greedy<<<1, kMergeThreads, 0, s>>>(a.x, a.z, a.circ, a.sigma, a.u, a.w, a.uvs, a.wvs,
-                                               n, threshold, G, keep, count);
+                                               n, threshold, G, alist, n_abs, keep, count);
     size_t tb = L.tmp_bytes;
     cub::DeviceScan::ExclusiveSum(b + L.tmp, tb, keep, pos, (int64_t)n, s);
     const int grid = sms * 4;
