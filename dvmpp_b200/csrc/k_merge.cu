@@ -167,15 +167,17 @@ __global__ void __launch_bounds__(kMergeThreads, 1)
                     }
                 }
             } else {
-                for (long long cz = cz0; cz <= cz1; ++cz)
-                    for (long long cx = cx0; cx <= cx1; ++cx) {
-                        const uint64_t c = (uint64_t)cz * G.nxc + cx;
-                        for (uint32_t q = G.cstart[c] + tid; q < G.cend[c]; q += kMergeThreads) {
-                            const uint32_t j = G.svals[q];
-                            if (j < j0 || j >= best || !keep[j]) continue;
-                            if (merge_test(xi, zi, gi, x[j], z[j], circ[j], thr)) best = j;
-                        }
+                // one warp per cell, so the cells' bounds are loaded concurrently
+                const long long ncx = cx1 - cx0 + 1, ncell = ncx * (cz1 - cz0 + 1);
+                const uint32_t warp = tid >> 5, lane = tid & 31;
+                for (long long k = warp; k < ncell; k += kMergeThreads / 32) {
+                    const uint64_t c = (uint64_t)(cz0 + k / ncx) * G.nxc + (cx0 + k % ncx);
+                    for (uint32_t q = G.cstart[c] + lane; q < G.cend[c]; q += 32) {
+                        const uint32_t j = G.svals[q];
+                        if (j < j0 || j >= best || !keep[j]) continue;
+                        if (merge_test(xi, zi, gi, x[j], z[j], circ[j], thr)) best = j;
                     }
+                }
                 for (uint32_t q = n_grid + tid; q < n; q += kMergeThreads) {
                     const uint32_t j = G.svals[q];
                     if (j < j0 || j >= best || !keep[j]) continue;
