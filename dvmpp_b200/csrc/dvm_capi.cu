@@ -956,6 +956,7 @@ int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const 
     }
     h.area = xmx - xmn;  // src/VortexSheet.cpp:74
     h.bxmax = xmx + 1e-9 * (1.0 + std::fabs(xmx));
+    h.bxmin = xmn - 1e-9 * (1.0 + std::fabs(xmn));
     h.bzmin = zmn;
     h.bzmax = zmx;
     const double L = std::max(xmx - xmn, zmx - zmn);

@@ -85,6 +85,7 @@ struct InstDesc {
     // scalars
     double rho, nu, dt, ux, uz, cutoff_exp, Ur, area;
     double bxmax, bzmin, bzmax;     // contour bounding box (x padded) for the crossing early-out
+    double bxmin;
     double kx0, kz0, kinv;          // Morton-key domain: cell = (x - kx0) * kinv
     uint32_t M;                     // max_NumPanelVort
     int np;

@@ -172,21 +172,27 @@ struct Body {
     int np;
 };
 
-// Crossing-number test, cn == 1 (src/VortexSheet.cpp:447-464).  Points outside
-// the contour's z-range, or to the right of its padded x-range, cross no edge.
-__device__ __forceinline__ bool inside_body(const double* __restrict__ xp,
-                                            const double* __restrict__ zp, int np, double xc,
-                                            double zc, double bxmax, double bzmin, double bzmax) {
-    if (zc < bzmin || zc >= bzmax || xc > bxmax) return false;
+// Crossing-number test, cn == 1 (src/VortexSheet.cpp:447-464), with the 32
+// lanes of a warp sharing one point's edges (every lane passes the same point;
+// the crossing count is an integer sum, so the result is the sequential
+// loop's).  Points outside the contour's z-range or x-range cross no edge or an
+// even number of them, so the bounding box settles them.
+__device__ __forceinline__ bool in_bbox(const InstDesc& d, double xc, double zc) {
+    return !(zc < d.bzmin || zc >= d.bzmax || xc > d.bxmax || xc < d.bxmin);
+}
+
+__device__ __forceinline__ bool inside_body_warp(const double* __restrict__ xp,
+                                                 const double* __restrict__ zp, int np,
+                                                 double xc, double zc) {
     int cn = 0;
-    for (int i = 0; i < np; ++i) {
+    for (int i = threadIdx.x & 31; i < np; i += 32) {
         const double z0 = zp[i], z1 = zp[i + 1];
         if (((z0 <= zc) && (z1 > zc)) || ((z0 > zc) && (z1 <= zc))) {
             const double vt = ddiv(dsub(zc, z0), dsub(z1, z0));
             if (xc < dadd(xp[i], dmul(vt, dsub(xp[i + 1], xp[i])))) ++cn;
         }
     }
-    return cn == 1;
+    return __reduce_add_sync(0xffffffffu, (unsigned)cn) == 1u;
 }
 
 __device__ __forceinline__ void load_contour(const InstDesc& d, double* sx, double* sz,
@@ -239,34 +245,55 @@ __global__ void __launch_bounds__(256) k_reflect(const InstDesc* __restrict__ ta
         if (threadIdx.x == 0) s_loaded = k;
         const uint32_t n = st[e.inst].n;
         const uint32_t i = (item - s_pre[k]) * 256 + threadIdx.x;
-        if (i < n) {
-            const double px = d.x[i], pz = d.z[i];
-            if (inside_body(sx, sz, np, px, pz, d.bxmax, d.bzmin, d.bzmax)) {
-                int cp = 0;
-                double md = 1e10;
-                for (int j = 0; j < np; ++j) {
-                    const double x0 = sx[j], z0 = sz[j], x1 = sx[j + 1], z1 = sz[j + 1];
-                    const double vx = dsub(px, x0), vz = dsub(pz, z0);
-                    const double dx = dsub(x1, x0), dz = dsub(z1, z0);
-                    const double len = dadd(dmul(dx, dx), dmul(dz, dz));
-                    double t = ddiv(dadd(dmul(vx, dx), dmul(vz, dz)), len);
-                    t = (t < 1.0) ? t : 1.0;  // std::min(1.0, t)
-                    t = (0.0 < t) ? t : 0.0;  // std::max(0.0, .)
-                    const double cx = dadd(x0, dmul(t, dx)), cz = dadd(z0, dmul(t, dz));
-                    const double ex = dsub(px, cx), ez = dsub(pz, cz);
-                    const double dist = sqrt(dadd(dmul(ex, ex), dmul(ez, ez)));
-                    if (dist < md) {
-                        md = dist;
-                        cp = j;
-                    }
+        const bool valid = i < n;
+        const double px = valid ? d.x[i] : 0.0, pz = valid ? d.z[i] : 0.0;
+        // blobs in the contour's bounding box, handled one at a time by the
+        // whole warp (edges and panels split over the lanes)
+        unsigned cand = __ballot_sync(0xffffffffu, valid && in_bbox(d, px, pz));
+        const int lane = threadIdx.x & 31;
+        while (cand) {
+            const int src = __ffs(cand) - 1;
+            cand &= cand - 1;
+            const double qx = __shfl_sync(0xffffffffu, px, src);
+            const double qz = __shfl_sync(0xffffffffu, pz, src);
+            if (!inside_body_warp(sx, sz, np, qx, qz)) continue;
+            // nearest panel: the first minimum of the clamped point-segment
+            // distance (src/VortexSheet.cpp:378-390), per lane over its
+            // panels in order, then the least (distance, panel) over the warp
+            int cp = 0;
+            double md = 1e10;
+            for (int j = lane; j < np; j += 32) {
+                const double x0 = sx[j], z0 = sz[j], x1 = sx[j + 1], z1 = sz[j + 1];
+                const double vx = dsub(qx, x0), vz = dsub(qz, z0);
+                const double dx = dsub(x1, x0), dz = dsub(z1, z0);
+                const double len = dadd(dmul(dx, dx), dmul(dz, dz));
+                double t = ddiv(dadd(dmul(vx, dx), dmul(vz, dz)), len);
+                t = (t < 1.0) ? t : 1.0;  // std::min(1.0, t)
+                t = (0.0 < t) ? t : 0.0;  // std::max(0.0, .)
+                const double cx = dadd(x0, dmul(t, dx)), cz = dadd(z0, dmul(t, dz));
+                const double ex = dsub(qx, cx), ez = dsub(qz, cz);
+                const double dist = sqrt(dadd(dmul(ex, ex), dmul(ez, ez)));
+                if (dist < md) {
+                    md = dist;
+                    cp = j;
                 }
-                const double off = dadd(dmul(2.0, md), 1e-6);
-                double nx = dadd(px, dmul(off, snx[cp]));
-                double nz = dadd(pz, dmul(off, snz[cp]));
-                if (inside_body(sx, sz, np, nx, nz, d.bxmax, d.bzmin, d.bzmax)) {
-                    nx = dadd(px, dmul(dmul(3.0, off), snx[cp]));
-                    nz = dadd(pz, dmul(dmul(3.0, off), snz[cp]));
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double m2 = __shfl_xor_sync(0xffffffffu, md, o);
+                const int c2 = __shfl_xor_sync(0xffffffffu, cp, o);
+                if (m2 < md || (m2 == md && c2 < cp)) {
+                    md = m2;
+                    cp = c2;
                 }
+            }
+            const double off = dadd(dmul(2.0, md), 1e-6);
+            double nx = dadd(qx, dmul(off, snx[cp]));
+            double nz = dadd(qz, dmul(off, snz[cp]));
+            if (inside_body_warp(sx, sz, np, nx, nz)) {
+                nx = dadd(qx, dmul(dmul(3.0, off), snx[cp]));
+                nz = dadd(qz, dmul(dmul(3.0, off), snz[cp]));
+            }
+            if (lane == src) {
                 d.x[i] = nx;
                 d.z[i] = nz;
             }
@@ -301,13 +328,25 @@ __global__ void __launch_bounds__(256) k_del_flags(const InstDesc* __restrict__ 
         if (threadIdx.x == 0) s_cnt = 0;
         __syncthreads();
         uint32_t mine = 0;
-        for (uint32_t q = threadIdx.x; q < kDelTile; q += blockDim.x) {
+        for (uint32_t q = threadIdx.x; q < kDelTile; q += blockDim.x) {  // uniform trip count
             const uint32_t i = t * kDelTile + q;
-            if (i >= n) break;
-            const uint8_t keep =
-                inside_body(sx, sz, d.np, d.x[i], d.z[i], d.bxmax, d.bzmin, d.bzmax) ? 0 : 1;
-            flags[e.coff + i] = keep;
-            mine += keep;
+            const bool valid = i < n;
+            const double px = valid ? d.x[i] : 0.0, pz = valid ? d.z[i] : 0.0;
+            // bounding-box candidates, tested by the whole warp one at a time
+            unsigned cand = __ballot_sync(0xffffffffu, valid && in_bbox(d, px, pz));
+            bool inside = false;
+            while (cand) {
+                const int src = __ffs(cand) - 1;
+                cand &= cand - 1;
+                const bool in = inside_body_warp(sx, sz, d.np, __shfl_sync(0xffffffffu, px, src),
+                                                 __shfl_sync(0xffffffffu, pz, src));
+                if ((threadIdx.x & 31) == src) inside = in;
+            }
+            if (valid) {
+                const uint8_t keep = inside ? 0 : 1;
+                flags[e.coff + i] = keep;
+                mine += keep;
+            }
         }
         for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
         if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, mine);
