@@ -328,6 +328,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
                  o_rhs = take(16 * rhs), o_circ = take(8 * circ + 8), o_cub = take(cub + 256),
                  o_work = take(64 * sizeof(unsigned)), o_flags = take(cap),
                  o_tiles = take(4 * (cap / 1024 + 1)),
+                 o_tbase = take(4 * (cap / 1024 + 1)), o_kept = take(4 * 1024),
                  o_comp = need_delete ? take(8 * 8 * cap) : take(8),
                  o_jobs = take(256 * lists);
     const uint64_t bytes = off;
@@ -357,6 +358,8 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     w.work = reinterpret_cast<unsigned*>(b + o_work);
     w.flags = reinterpret_cast<uint8_t*>(b + o_flags);
     w.tile_counts = reinterpret_cast<uint32_t*>(b + o_tiles);
+    w.tile_base = reinterpret_cast<uint32_t*>(b + o_tbase);
+    w.del_kept = reinterpret_cast<uint32_t*>(b + o_kept);
     w.compact = need_delete ? reinterpret_cast<double*>(b + o_comp) : nullptr;
     w.jobs = b + o_jobs;
     c->ws_cap = cap;
@@ -492,7 +495,7 @@ void issue_step(dvm_ctx* c, Plan& pl) {
         p = prof_begin(c, DVM_PROF_CROSS);
         delete_inside(T, S, pl.del.d_list, pl.del.n, pl.del.max_np, ws, sms, s);
         prof_end(c, p);
-        L += 4;
+        L += 5;
     }
     p = prof_begin(c, DVM_PROF_LOADS);
     loads(T, S, pl.all.d_list, pl.all.n, pl.all.max_np, s);

@@ -145,6 +145,8 @@ struct Workspace {
     unsigned* work = nullptr;      // 16 dynamic work counters
     uint8_t* flags = nullptr;      // delete: keep flags, total_cap
     uint32_t* tile_counts = nullptr;  // delete: kept per 1024-tile, total_cap / 1024
+    uint32_t* tile_base = nullptr;    // delete: exclusive prefix of tile_counts, per simulation
+    uint32_t* del_kept = nullptr;     // delete: kept blobs per list entry
     double* compact = nullptr;     // delete: 9 * total_cap words of staging
     void* jobs = nullptr;          // per-entry job records (256 B each)
     int key_bits = 40;

@@ -9,6 +9,8 @@
 // per operation, and DELETE is a stable (order-preserving) compaction.
 #include <cfloat>
 
+#include <cub/cub.cuh>
+
 #include "dvm_device.cuh"
 #include "dvm_internal.h"
 
@@ -356,37 +358,54 @@ __global__ void __launch_bounds__(256) k_del_flags(const InstDesc* __restrict__ 
     }
 }
 
+// Per simulation (one block each): exclusive prefix of the kept counts of its
+// 1024-tiles, and the total kept.
+__global__ void __launch_bounds__(1024) k_del_scan(const InstState* __restrict__ st,
+                                                   const ListEntry* __restrict__ list,
+                                                   const uint32_t* __restrict__ tile_counts,
+                                                   uint32_t* __restrict__ tile_base,
+                                                   uint32_t* __restrict__ del_kept) {
+    using Scan = cub::BlockScan<uint32_t, 1024>;
+    __shared__ typename Scan::TempStorage tmp;
+    const ListEntry e = list[blockIdx.x];
+    const InstState& S = st[e.inst];
+    if (S.status) return;
+    const uint32_t ntiles = (S.n + kDelTile - 1) / kDelTile;
+    const uint32_t* tc = tile_counts + e.coff / kDelTile;
+    uint32_t* tb = tile_base + e.coff / kDelTile;
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < ntiles; c0 += 1024) {
+        const uint32_t t = c0 + threadIdx.x;
+        uint32_t v = t < ntiles ? tc[t] : 0u, ex = 0, agg = 0;
+        Scan(tmp).ExclusiveSum(v, ex, agg);
+        if (t < ntiles) tb[t] = carry + ex;
+        carry += agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) del_kept[blockIdx.x] = carry;
+}
+
 // Stable scatter of kept blobs into the staging area (8 FP64 arrays + ids).
 __global__ void __launch_bounds__(kDelTile) k_del_compact(const InstDesc* __restrict__ table,
                                                           const InstState* __restrict__ st,
                                                           const ListEntry* __restrict__ list,
                                                           const uint8_t* __restrict__ flags,
-                                                          const uint32_t* __restrict__ tile_counts,
+                                                          const uint32_t* __restrict__ tile_base,
+                                                          const uint32_t* __restrict__ del_kept,
                                                           double* __restrict__ stage,
                                                           uint64_t total_cap) {
     __shared__ uint32_t s_warp[kDelTile / 32];
-    __shared__ uint32_t s_base, s_kept;
+    __shared__ uint32_t s_base;
     const ListEntry e = list[blockIdx.y];
     const InstDesc& d = table[e.inst];
     const InstState& S = st[e.inst];
     if (S.status) return;
     const uint32_t n = S.n;
     const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
-    const uint32_t* tc = tile_counts + e.coff / kDelTile;
-    if (threadIdx.x == 0) {
-        uint32_t kept = 0;
-        for (uint32_t t = 0; t < ntiles; ++t) kept += tc[t];
-        s_kept = kept;
-    }
-    __syncthreads();
-    if (s_kept == n) return;  // nothing deleted: the reference returns early (:420-422)
+    const uint32_t* tb = tile_base + e.coff / kDelTile;
+    if (del_kept[blockIdx.y] == n) return;  // nothing deleted: the reference returns early (:420-422)
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (threadIdx.x == 0) {
-            uint32_t b = 0;
-            for (uint32_t q = 0; q < t; ++q) b += tc[q];
-            s_base = b;
-        }
-        const uint32_t i = t * kDelTile + threadIdx.x;
+        if (threadIdx.x == 0) s_base = tb[t];        const uint32_t i = t * kDelTile + threadIdx.x;
         const uint32_t keep = (i < n) ? flags[e.coff + i] : 0u;
         const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
         const uint32_t ball = __ballot_sync(0xffffffffu, keep);
@@ -419,23 +438,14 @@ __global__ void __launch_bounds__(kDelTile) k_del_compact(const InstDesc* __rest
 
 __global__ void k_del_copyback(const InstDesc* __restrict__ table, InstState* __restrict__ st,
                                const ListEntry* __restrict__ list,
-                               const uint32_t* __restrict__ tile_counts,
+                               const uint32_t* __restrict__ del_kept,
                                const double* __restrict__ stage, uint64_t total_cap) {
     const ListEntry e = list[blockIdx.y];
     const InstDesc& d = table[e.inst];
     const InstState& S = st[e.inst];
     if (S.status) return;
     const uint32_t n = S.n;
-    const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
-    const uint32_t* tc = tile_counts + e.coff / kDelTile;
-    __shared__ uint32_t s_kept;
-    if (threadIdx.x == 0) {
-        uint32_t kept = 0;
-        for (uint32_t t = 0; t < ntiles; ++t) kept += tc[t];
-        s_kept = kept;
-    }
-    __syncthreads();
-    const uint32_t kept = s_kept;
+    const uint32_t kept = del_kept[blockIdx.y];
     if (kept == n) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kept; i += gridDim.x * blockDim.x) {
         const uint64_t o = e.coff + i;
@@ -452,16 +462,12 @@ __global__ void k_del_copyback(const InstDesc* __restrict__ table, InstState* __
 }
 
 __global__ void k_del_finish(InstState* __restrict__ st, const ListEntry* __restrict__ list,
-                             int nlist, const uint32_t* __restrict__ tile_counts) {
+                             int nlist, const uint32_t* __restrict__ del_kept) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nlist) return;
-    const ListEntry e = list[k];
-    InstState& S = st[e.inst];
+    InstState& S = st[list[k].inst];
     if (S.status) return;
-    const uint32_t ntiles = (S.n + kDelTile - 1) / kDelTile;
-    uint32_t kept = 0;
-    for (uint32_t t = 0; t < ntiles; ++t) kept += tile_counts[e.coff / kDelTile + t];
-    S.n = kept;
+    S.n = del_kept[k];
 }
 
 size_t contour_smem(int max_np) { return sizeof(double) * (4 * (size_t)max_np + 2); }
@@ -509,11 +515,12 @@ void delete_inside(const InstDesc* table, InstState* st, const ListEntry* list, 
     }
     const int gx = std::max(1, sms * 4 / std::max(1, nlist));
     k_del_flags<<<dim3(gx, nlist), 256, smem, s>>>(table, st, list, ws.flags, ws.tile_counts);
-    k_del_compact<<<dim3(gx, nlist), kDelTile, 0, s>>>(table, st, list, ws.flags, ws.tile_counts,
-                                                       ws.compact, ws.total_cap);
-    k_del_copyback<<<dim3(gx, nlist), 256, 0, s>>>(table, st, list, ws.tile_counts, ws.compact,
+    k_del_scan<<<nlist, 1024, 0, s>>>(st, list, ws.tile_counts, ws.tile_base, ws.del_kept);
+    k_del_compact<<<dim3(gx, nlist), kDelTile, 0, s>>>(table, st, list, ws.flags, ws.tile_base,
+                                                       ws.del_kept, ws.compact, ws.total_cap);
+    k_del_copyback<<<dim3(gx, nlist), 256, 0, s>>>(table, st, list, ws.del_kept, ws.compact,
                                                    ws.total_cap);
-    k_del_finish<<<(nlist + 127) / 128, 128, 0, s>>>(st, list, nlist, ws.tile_counts);
+    k_del_finish<<<(nlist + 127) / 128, 128, 0, s>>>(st, list, nlist, ws.del_kept);
 }
 
 }  // namespace dvmk
