@@ -477,7 +477,8 @@ size_t contour_smem(int max_np) { return sizeof(double) * (4 * (size_t)max_np + 
 void diffuse(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
              const Workspace& ws, int sms, cudaStream_t s) {
     (void)ws;
-    dim3 g(std::max(1, sms * 8 / std::max(1, nlist)), nlist);
+    // many resident warps: each blob is a chain of FP64 log / sqrt / sincos
+    dim3 g(std::max(1, sms * 32 / std::max(1, nlist)), nlist);
     k_diffuse<<<g, 256, 0, s>>>(table, st, list, nlist);
 }
 
