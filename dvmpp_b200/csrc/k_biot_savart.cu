@@ -189,9 +189,7 @@ __device__ __forceinline__ uint32_t chunk_size(uint32_t n, int chunks) {
 // items) or 4 (128-target items); the choice changes which targets share a
 // warp, never a target's own operation sequence, so results do not depend on it.
 constexpr int kWWarps = 4;            // independent warps per block
-#ifndef DVM_SELF_MINBLOCKS
-#define DVM_SELF_MINBLOCKS 3          // blocks per SM the register budget is sized for
-#endif
+constexpr int kSelfMinBlocks = 3;     // blocks per SM the 256-target variant's registers allow
 
 // Packed FP32x2 arithmetic (sm_100): one instruction operates on a pair of
 // targets, halving the issue slots of the pair loop; each half is rounded
@@ -234,15 +232,7 @@ struct StagedSrc {
     float4 b;
 };
 
-// Target pairs (of WR / 2 per lane) whose two reciprocals share one MUFU.RCP.
-#ifndef DVM_PAIR_RCP
-#define DVM_PAIR_RCP 0
-#endif
-constexpr int kPairRcp = DVM_PAIR_RCP;
-#ifndef DVM_FAR_UNROLL
-#define DVM_FAR_UNROLL 8
-#endif
-constexpr int kFarUnroll = DVM_FAR_UNROLL;  // sources per unrolled far-loop body
+constexpr int kFarUnroll = 8;  // sources per unrolled far-loop body
 
 // Far pairs: no core test.  Accumulates -u (so every update is one FMA) and w.
 template <int WP>
@@ -259,17 +249,8 @@ __device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
             const uint64_t dx = f2sub(tx2[q], sx);
             const uint64_t dz = f2sub(tz2[q], sz);
             const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
-            uint64_t inv;
-            if (q < kPairRcp) {
-                // one MUFU for both halves: 1/(a b) * b = 1/a, 1/(a b) * a = 1/b.
-                // Far pairs have 10 sigma^2 <= r2 <~ 1e4 (item-relative), so a*b
-                // stays normal; padded sources give rcp(inf) = 0 and Gamma = 0.
-                const float a = f2lo(r2), b = f2hi(r2);
-                const float ip = rcp_approx(a * b);
-                inv = f2pack(b * ip, a * ip);
-            } else {
-                inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
-            }
+            // one MUFU reciprocal per pair (padded sources: rcp of ~2e36, Gamma 0)
+            const uint64_t inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
             const uint64_t g = f2mul(inv, sg);
             nu2[q] = f2fma(g, dz, nu2[q]);
             w2[q] = f2fma(g, dx, w2[q]);
@@ -791,7 +772,7 @@ void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* 
             k_self_f32<4, 4><<<g, 32 * kWWarps, 0, s>>>(st, list, nlist, pxz, pf, ws.meta,
                                                          ws.part, ws.work);
         else
-            k_self_f32<8, DVM_SELF_MINBLOCKS><<<g, 32 * kWWarps, 0, s>>>(
+            k_self_f32<8, kSelfMinBlocks><<<g, 32 * kWWarps, 0, s>>>(
                 st, list, nlist, pxz, pf, ws.meta, ws.part, ws.work);
     } else {
         k_self_f64<<<sms, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part, ws.work);
