@@ -208,13 +208,22 @@ class RefModel:
         self.acc["d"].append((t["diff"] + t["cross"]) / max(N, 1))
         self.acc["e"].append((t["rel"] + t["loads"]) / max(Np, 1))
 
-    def step_time(self, instances) -> float:
+    def phase_times(self, instances) -> dict:
+        """Seconds per batched step by phase of DVMBase::compute_step."""
         r = {k: float(np.mean(v)) for k, v in self.acc.items()}
-        tot = 0.0
+        out = {"biotsavart_N2": 0.0, "vortexsheetbc_NNp": 0.0, "solve_and_update_NNp": 0.0,
+               "diffusion_and_crossing_N": 0.0, "release_and_loads_Np": 0.0}
         for inst in instances:
             N, Np = inst["nblobs"], inst["npanels"]
-            tot += r["a"] * N * N + (r["b"] + r["c"]) * N * Np + r["d"] * N + r["e"] * Np
-        return tot
+            out["biotsavart_N2"] += r["a"] * N * N
+            out["vortexsheetbc_NNp"] += r["b"] * N * Np
+            out["solve_and_update_NNp"] += r["c"] * N * Np
+            out["diffusion_and_crossing_N"] += r["d"] * N
+            out["release_and_loads_Np"] += r["e"] * Np
+        return out
+
+    def step_time(self, instances) -> float:
+        return sum(self.phase_times(instances).values())
 
 
 def ref_sample_step(ref, inst, workdir):
@@ -274,7 +283,7 @@ def reference_sample(instances, n_samples: int, spread: bool = False):
             model.add(inst["nblobs"], inst["npanels"], tt)
     batch = model.step_time(instances)
     return {"batch_step_s": batch, "sampled": [instances[k]["nblobs"] for k in pick],
-            "wall_s": total}
+            "wall_s": total, "phases_s": model.phase_times(instances)}
 
 
 def run_reference_arm(args, dist):
@@ -293,10 +302,12 @@ def run_reference_arm(args, dist):
         reference_sample(instances, 1)
     times = []
     sampled = []
+    phases = []
     for k in range(args.steps):
         r = reference_sample(instances, 1 + (k % 2))
         times.append(r["batch_step_s"])
         sampled.append(r["sampled"])
+        phases.append(r["phases_s"])
     step_s = float(np.median(times))
     value = args.instances / step_s
     line = {
@@ -311,7 +322,9 @@ def run_reference_arm(args, dist):
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": _cores(), "kind": kind,
                          "sample": "each step: one reference DVMBase::compute_step, phase-timed, "
                                    "on the 1-2 smallest instances; per-phase rates extrapolated "
-                                   "to all 64 instances by N^2, N*Np, N, Np"},
+                                   "to all 64 instances by N^2, N*Np, N, Np",
+                         "s_per_step_by_phase": {k: float(np.median([p[k] for p in phases]))
+                                                 for k in phases[0]} if phases else {}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -504,7 +517,8 @@ def run_ours(args, dist):
                    "sample": f"one reference compute_step (phase-timed) on each of 3 "
                              f"instances from the smallest to the median (N={r['sampled']}), per-phase rates "
                              f"extrapolated to all {args.instances} instances; output writing "
-                             f"off; {r['wall_s']:.1f} s of CPU work"}
+                             f"off; {r['wall_s']:.1f} s of CPU work",
+                   "s_per_step_by_phase": r["phases_s"]}
 
     nblobs = [s.n for s in sims]
     line = {
