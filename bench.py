@@ -570,7 +570,9 @@ def run_ours(args, dist):
 
     # ---- the standalone N-body configuration (N = 2^20 wake) and the serving
     # loop (continuous batching vs the plain serial path): reported beside
-    if args.nbody_n:
+    # (single-GPU runs only: these legs use device 0 and are not part of the
+    # replicated job)
+    if args.nbody_n and dist.world == 1:
         from dvmpp_b200 import cases
 
         nb = cases.run_nbody(args.nbody_n, [N.F32], 2)
@@ -578,7 +580,7 @@ def run_ours(args, dist):
         line["nbody"] = {"n": args.nbody_n, "pair_kernel_ms": r["pair_kernel_ms"],
                          "gpairs_per_s": r["gpairs_per_s"], "tflops_12_per_pair": r["tflops_12_per_pair"],
                          "fp32_peak_frac": r["fp32_peak_frac"]}
-    if args.serve_requests:
+    if args.serve_requests and dist.world == 1:
         from dvmpp_b200 import cases
 
         keys = ("sim_steps_per_s", "latency_p50_s", "latency_p95_s", "latency_p99_s",
