@@ -479,22 +479,19 @@ def run_ours(args, dist):
         ctx.sync()
         t0 = time.perf_counter()
         sizes = generate(hbuf[0])
-        for sm, hb, k in zip(sims, hbuf[0], sizes):
-            sm.push_uniforms(hb[:k])
-            h2d += 8 * k
+        ctx.batch_push_uniforms(sims, hbuf[0], sizes)  # one wait for all simulations
+        h2d += 8 * sum(sizes)
         for step in range(args.e2e_steps):
             ctx.step_batch(sims, 1, use_graph=True)  # asynchronous
             last = step + 1 == args.e2e_steps
             if not last:
                 sizes = generate(hbuf[(step + 1) % 2])  # overlaps the GPU step
-            for i, (sm, ox, oz, oc) in enumerate(zip(sims, out_x, out_z, out_c)):
-                nprev[i] = sm.get_state_into(ox, oz, oc)
-                sm.loads()
-                d2h += 3 * 8 * sm.last_n + 4 * 8
+            # x, z, circ of every blob and the loads of every simulation, one wait
+            nprev, loads = ctx.batch_get_state(sims, out_x, out_z, out_c)
+            d2h += sum(3 * 8 * n + 4 * 8 for n in nprev)
             if not last:
-                for sm, hb, k in zip(sims, hbuf[(step + 1) % 2], sizes):
-                    sm.push_uniforms(hb[:k])
-                    h2d += 8 * k
+                ctx.batch_push_uniforms(sims, hbuf[(step + 1) % 2], sizes)
+                h2d += 8 * sum(sizes)
         ctx.sync()
         e2e_s = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.world * args.instances * args.e2e_steps / e2e_s, "unit": UNIT,

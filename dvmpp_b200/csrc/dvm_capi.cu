@@ -1222,11 +1222,9 @@ int dvm_sim_rng_position(dvm_sim* s, uint64_t* consumed, uint64_t* avail) {
     return DVM_OK;
 }
 
-int dvm_batch_status(dvm_ctx* c, dvm_sim* const* sims, int nsims, int32_t* status) {
-    if (!c || nsims < 0 || (nsims && (!sims || !status))) return fail(DVM_ERR_ARG, "bad argument");
-    if (nsims == 0) return DVM_OK;
-    std::lock_guard<std::mutex> lk(c->mu);
-    CK(cudaSetDevice(c->device));
+// The listed simulations' InstState rows into c->h_state: one copy, one wait.
+// Call with c->mu held.
+static int read_states(dvm_ctx* c, dvm_sim* const* sims, int nsims) {
     int hi = 0;
     for (int i = 0; i < nsims; ++i) {
         if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
@@ -1236,12 +1234,22 @@ int dvm_batch_status(dvm_ctx* c, dvm_sim* const* sims, int nsims, int32_t* statu
         if (c->h_state) cudaFreeHost(c->h_state);
         c->h_state = nullptr;
         c->h_state_slots = 0;
-        CK(cudaMallocHost(&c->h_state, sizeof(InstState) * (size_t)hi));
-        c->h_state_slots = hi;
+        CK(cudaMallocHost(&c->h_state, sizeof(InstState) * (size_t)kTableCap));
+        c->h_state_slots = kTableCap;
     }
     CK(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(InstState) * (size_t)hi,
                        cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return DVM_OK;
+}
+
+int dvm_batch_status(dvm_ctx* c, dvm_sim* const* sims, int nsims, int32_t* status) {
+    if (!c || nsims < 0 || (nsims && (!sims || !status))) return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    const int rc = read_states(c, sims, nsims);
+    if (rc) return rc;
     for (int i = 0; i < nsims; ++i) {
         const int st = c->h_state[sims[i]->slot].status;
         status[i] = st == 0 ? DVM_OK
@@ -1249,6 +1257,78 @@ int dvm_batch_status(dvm_ctx* c, dvm_sim* const* sims, int nsims, int32_t* statu
                   : st == kErrRelease ? DVM_ERR_RELEASE
                   : st == kErrRngExhausted ? DVM_ERR_RNG : st;
     }
+    return DVM_OK;
+}
+
+int dvm_batch_get_state(dvm_ctx* c, dvm_sim* const* sims, int nsims, double* const* x,
+                        double* const* z, double* const* circ, const uint64_t* caps,
+                        uint64_t* counts, double* loads) {
+    if (!c || nsims < 0 || (nsims && (!sims || !counts))) return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    int rc = read_states(c, sims, nsims);
+    if (rc) return rc;
+    for (int i = 0; i < nsims; ++i) {
+        const InstState& S = c->h_state[sims[i]->slot];
+        const uint64_t n = S.n;
+        counts[i] = n;
+        if (loads) {
+            loads[4 * i] = S.fx;
+            loads[4 * i + 1] = S.fz;
+            loads[4 * i + 2] = S.cd;
+            loads[4 * i + 3] = S.cl;
+        }
+        const bool any = (x && x[i]) || (z && z[i]) || (circ && circ[i]);
+        if (!any || n == 0) continue;
+        if (!caps || n > caps[i])
+            return fail(DVM_ERR_ARG, "output capacity smaller than the blob count");
+        const InstDesc& h = sims[i]->h;
+        if (x && x[i]) CK(cudaMemcpyAsync(x[i], h.x, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+        if (z && z[i]) CK(cudaMemcpyAsync(z[i], h.z, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+        if (circ && circ[i])
+            CK(cudaMemcpyAsync(circ[i], h.circ, 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return DVM_OK;
+}
+
+int dvm_batch_push_uniforms(dvm_ctx* c, dvm_sim* const* sims, int nsims, const double* const* u,
+                            const uint64_t* counts) {
+    if (!c || nsims < 0 || (nsims && (!sims || !u || !counts)))
+        return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    int rc = read_states(c, sims, nsims);
+    if (rc) return rc;
+    const uint64_t zero = 0;
+    for (int i = 0; i < nsims; ++i) {
+        dvm_sim* s = sims[i];
+        const uint64_t n = counts[i];
+        if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
+        if (n && !u[i]) return fail(DVM_ERR_ARG, "null uniform array");
+        const uint64_t cursor = c->h_state[s->slot].cursor;
+        uint64_t count = s->h.ucount;
+        if (count + n > s->ucap) {  // drop the consumed prefix (as dvm_sim_push_uniforms)
+            const uint64_t keep = count - cursor;
+            if (keep + n > s->ucap) return fail(DVM_ERR_CAPACITY, "uniform buffer too small");
+            if (keep && cursor)
+                CK(cudaMemcpyAsync(s->uniforms, s->uniforms + cursor, 8 * keep,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+            s->consumed_base += cursor;
+            count = keep;
+            CK(cudaMemcpyAsync(&c->d_state[s->slot].cursor, &zero, 8, cudaMemcpyHostToDevice,
+                               c->stream));
+        }
+        if (n)
+            CK(cudaMemcpyAsync(s->uniforms + count, u[i], 8 * n, cudaMemcpyHostToDevice,
+                               c->stream));
+        s->h.ucount = count + n;
+        rc = upload_desc(s);
+        if (rc) return rc;
+    }
+    CK(cudaStreamSynchronize(c->stream));
     return DVM_OK;
 }
 

@@ -278,6 +278,32 @@ class Context:
                 "default_ms": r.default_ms,
                 "candidates": [dict(c, ms=r.ms[k]) for k, c in enumerate(cands[:r.candidates])]}
 
+    def batch_get_state(self, sims, xs=None, zs=None, cs=None):
+        """Blob counts and loads of many simulations with one wait; x / z / circ
+        copied into the given buffers (lists of float64 arrays, e.g. pinned).
+        Returns (counts, loads[nsims, 4])."""
+        n = len(sims)
+        P = C.POINTER(C.c_double)
+
+        def ptrs(bufs):
+            return None if bufs is None else (P * n)(*[_p(b) for b in bufs])
+
+        given = [arr for arr in (xs, zs, cs) if arr is not None]
+        caps = (C.c_uint64 * n)(*[min(a[i].size for a in given) if given else 0
+                                  for i in range(n)])
+        counts = (C.c_uint64 * n)()
+        loads = np.empty((n, 4))
+        _check(self.lib.dvm_batch_get_state(self.h, self._sim_array(sims), n, ptrs(xs), ptrs(zs),
+                                            ptrs(cs), caps, counts, _p(loads)))
+        return [int(counts[i]) for i in range(n)], loads
+
+    def batch_push_uniforms(self, sims, bufs, counts):
+        n = len(sims)
+        P = C.POINTER(C.c_double)
+        arr = (P * n)(*[_p(b) for b in bufs])
+        cnt = (C.c_uint64 * n)(*[int(k) for k in counts])
+        _check(self.lib.dvm_batch_push_uniforms(self.h, self._sim_array(sims), n, arr, cnt))
+
     def batch_status(self, sims) -> list:
         out = (C.c_int32 * max(len(sims), 1))()
         _check(self.lib.dvm_batch_status(self.h, self._sim_array(sims), len(sims), out))
@@ -558,6 +584,11 @@ SIGNATURES.update({
     "dvm_ctx_tuning_table": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
                                        C.POINTER(PairConfig), C.POINTER(C.c_int)]),
     "dvm_batch_status": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int32)]),
+    "dvm_batch_get_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                      _dp]),
+    "dvm_batch_push_uniforms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                          C.POINTER(C.c_uint64)]),
     "dvm_sim_probe": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]),
     "dvm_sim_merge": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_uint64)]),
     "dvm_merge_blobs": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _u32p,

@@ -301,6 +301,17 @@ int dvm_step_batch(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int nsteps, in
 /* Device status of every listed simulation with one copy and one wait (what
  * dvm_sim_status returns, per simulation, into status[i]). */
 int dvm_batch_status(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, int32_t* status);
+/* Read back many simulations with one wait: counts[i] = blob count; x[i], z[i],
+ * circ[i] (any of the three arrays, or entries, may be null) receive the first
+ * counts[i] values (DVM_ERR_ARG if counts[i] > caps[i]); loads (may be null)
+ * gets fx, fz, Cd, Cl per simulation.  What DVMBase::write_outputs consumes. */
+int dvm_batch_get_state(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, double* const* x,
+                        double* const* z, double* const* circ, const uint64_t* caps,
+                        uint64_t* counts, double* loads);
+/* dvm_sim_push_uniforms for many simulations with one wait (u[i]: counts[i]
+ * values for simulation i). */
+int dvm_batch_push_uniforms(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, const double* const* u,
+                            const uint64_t* counts);
 
 /* ---- pair-kernel autotuning (no counterpart in the reference) ---------------------
  * The FP32 blob-on-blob kernel's launch shape: targets per work item, persistent

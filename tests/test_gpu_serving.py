@@ -54,3 +54,41 @@ def test_admission_respects_hbm_budget(ctx):
     assert st["completed"] == len(reqs)
     assert st["peak_bytes"] <= budget
     assert 1 <= st["peak_active"] <= 3
+
+
+def test_batch_state_and_uniform_calls_match_single(ctx):
+    """dvm_batch_push_uniforms / dvm_batch_get_state against the per-simulation
+    calls: same trajectories, same counts, positions and loads."""
+    rng = np.random.default_rng(8)
+    bodies = [W.circle(64), W.ellipse(96, 0.5, 0.25, 5.0), W.circle(128)]
+
+    def make():
+        out = []
+        for k, (bx, bz) in enumerate(bodies):
+            s = ctx.sim(N.Params(capacity=1 << 15, rng_capacity=1 << 18, seed=k), bx, bz)
+            x, z, g, sg = W.wake(2000 + 500 * k, k, W.core_size(bx, bz))
+            s.set_blobs(x, z, g, sg)
+            out.append(s)
+        return out
+
+    a, b = make(), make()
+    for step in range(3):
+        us = [1.0 - rng.random(2 * s.n + 8 * s.np + 64) for s in a]
+        for s, u in zip(a, us):
+            s.push_uniforms(u)
+        ctx.batch_push_uniforms(b, us, [u.size for u in us])
+        ctx.step_batch(a, 1)
+        ctx.step_batch(b, 1)
+        xs = [np.empty(1 << 15) for _ in b]
+        zs = [np.empty(1 << 15) for _ in b]
+        cs = [np.empty(1 << 15) for _ in b]
+        counts, loads = ctx.batch_get_state(b, xs, zs, cs)
+        for i, s in enumerate(a):
+            d = s.blobs()
+            assert counts[i] == s.n
+            assert np.array_equal(xs[i][:counts[i]], d["x"])
+            assert np.array_equal(cs[i][:counts[i]], d["circ"])
+            assert np.allclose(loads[i], s.loads(), rtol=0, atol=0)
+    for s in a + b:
+        s.check()
+        s.close()
