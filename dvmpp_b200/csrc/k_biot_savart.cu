@@ -583,6 +583,7 @@ template <bool F32>
 __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int njobs) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ double s_x[256], s_z[256], s_c[256], s_thr[256], s_rs[256];
+    __shared__ float s_cf[256], s_thrf[256], s_rsf[256];  // FP32 copies (F32 path)
     __shared__ double s_red[8];
     if (threadIdx.x == 0) {
         unsigned acc = 0;
@@ -618,6 +619,11 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                 s_c[threadIdx.x] = J.sc[j];
                 s_thr[threadIdx.x] = dmul(10.0, s2);
                 s_rs[threadIdx.x] = ddiv(1.0, s2);
+                if (F32) {  // converted once per source instead of once per pair
+                    s_cf[threadIdx.x] = (float)s_c[threadIdx.x];
+                    s_thrf[threadIdx.x] = (float)s_thr[threadIdx.x];
+                    s_rsf[threadIdx.x] = (float)s_rs[threadIdx.x];
+                }
                 if (ttile == 0) csum += J.sc[j];
             }
             __syncthreads();
@@ -632,8 +638,8 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                     const float r2 = fmaf(dx, dx, dz * dz);
                     if (J.skip_close && !(r2 > 1e-15f)) continue;
                     float K = rcp_approx(r2);
-                    if (r2 < (float)s_thr[jj]) K = core_kernel(r2, (float)s_rs[jj], K);
-                    const float g = K * (float)s_c[jj];
+                    if (r2 < s_thrf[jj]) K = core_kernel(r2, s_rsf[jj], K);
+                    const float g = K * s_cf[jj];
                     kahan(su, cu, -g * dz);
                     kahan(sw, cw, g * dx);
                 }
