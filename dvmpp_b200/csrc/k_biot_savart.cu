@@ -238,6 +238,10 @@ struct StagedSrc {
 constexpr int kFarUnroll = 8;  // sources per unrolled far-loop body
 
 // Far pairs: no core test.  Accumulates -u (so every update is one FMA) and w.
+// (Sharing one reciprocal between the two targets of a packed pair, 1/a = b/(ab),
+// trades one MUFU operation for three FP32 multiplications; it measured 1-4 %
+// slower for 1/8 to 1/2 of the sources, the FMA pipe being nearly as loaded as
+// the MUFU pipe.)
 template <int WP>
 __device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
                                           const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
@@ -328,7 +332,6 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
                unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ StagedSrc s_src[kWWarps][kBsST];
-    __shared__ double s_box[kWWarps][4];
     constexpr int kWP = WR / 2, kWTT = 32 * WR;
     if (threadIdx.x == 0) {
         unsigned acc = 0;
@@ -363,43 +366,27 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
         const double2 o = X[t0 - t0 % 256u];
 
         uint64_t tx2[kWP], tz2[kWP];
-        double wxmin = DBL_MAX, wxmax = -DBL_MAX, wzmin = DBL_MAX, wzmax = -DBL_MAX;
         const uint32_t tb = t0 + lane * WR;
 #pragma unroll
         for (int q = 0; q < kWP; ++q) {
             float xs[2], zs[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                xs[h] = 0.0f;
+                xs[h] = 0.0f;  // padding targets sit on the origin (a real target)
                 zs[h] = 0.0f;
                 const uint32_t t = tb + 2 * q + h;
                 if (t < n) {
                     const double2 p = X[t];
                     xs[h] = (float)(p.x - o.x);
                     zs[h] = (float)(p.y - o.y);
-                    wxmin = fmin(wxmin, p.x);
-                    wxmax = fmax(wxmax, p.x);
-                    wzmin = fmin(wzmin, p.y);
-                    wzmax = fmax(wzmax, p.y);
                 }
             }
             tx2[q] = f2pack(xs[0], xs[1]);
             tz2[q] = f2pack(zs[0], zs[1]);
         }
-#pragma unroll
-        for (int q = 16; q > 0; q >>= 1) {
-            wxmin = fmin(wxmin, __shfl_xor_sync(0xffffffffu, wxmin, q));
-            wxmax = fmax(wxmax, __shfl_xor_sync(0xffffffffu, wxmax, q));
-            wzmin = fmin(wzmin, __shfl_xor_sync(0xffffffffu, wzmin, q));
-            wzmax = fmax(wzmax, __shfl_xor_sync(0xffffffffu, wzmax, q));
-        }
-        // the warp's target box lives in shared memory (registers go to the pair loop)
-        if (lane == 0) {
-            s_box[wid][0] = wxmin;
-            s_box[wid][1] = wxmax;
-            s_box[wid][2] = wzmin;
-            s_box[wid][3] = wzmax;
-        }
+        // The near/far test uses the box of the enclosing 256-target block
+        // (its sort tile), the same for every item shape.
+        const TileMeta& tm = meta[(e.coff + t0) / kBsST];
         float su[WR], cu[WR], sw[WR], cw[WR];  // Kahan sums of -u and w
 #pragma unroll
         for (int r = 0; r < WR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
@@ -424,8 +411,8 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
             }
             __syncwarp();
             const TileMeta m = meta[(e.coff + s0) / kBsST];
-            const double gx = fmax(0.0, fmax(m.xmin - s_box[wid][1], s_box[wid][0] - m.xmax));
-            const double gz = fmax(0.0, fmax(m.zmin - s_box[wid][3], s_box[wid][2] - m.zmax));
+            const double gx = fmax(0.0, fmax(m.xmin - tm.xmax, tm.xmin - m.xmax));
+            const double gz = fmax(0.0, fmax(m.zmin - tm.zmax, tm.zmin - m.zmax));
             uint64_t nu2[kWP], w2[kWP];
 #pragma unroll
             for (int q = 0; q < kWP; ++q) nu2[q] = w2[q] = 0ull;  // +0.0f in both halves
