@@ -276,44 +276,31 @@ __device__ __forceinline__ float core_kernel(float r2, float rs, float rcp_r2) {
     return r2 > 1e-30f ? -e * rcp_r2 : rs;
 }
 
-// Near pairs: the reference's exact test per pair (scalar; rare).
+// Near pairs: the reference's exact test per pair.  The shared arithmetic is
+// packed like the far path (each half rounds like the scalar instruction, so a
+// pair gets the same bits on either path); only the core kernel runs per pair.
 template <int WP>
 __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
                                            const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                            uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
-    constexpr int WR = 2 * WP;
-    float nu[WR], w[WR], tx[WR], tz[WR];
-#pragma unroll
-    for (int q = 0; q < WP; ++q) {
-        tx[2 * q] = f2lo(tx2[q]);
-        tx[2 * q + 1] = f2hi(tx2[q]);
-        tz[2 * q] = f2lo(tz2[q]);
-        tz[2 * q + 1] = f2hi(tz2[q]);
-        nu[2 * q] = f2lo(nu2[q]);
-        nu[2 * q + 1] = f2hi(nu2[q]);
-        w[2 * q] = f2lo(w2[q]);
-        w[2 * q + 1] = f2hi(w2[q]);
-    }
-#pragma unroll 1
+#pragma unroll 2
     for (int jj = 0; jj < kBsST; ++jj) {
         const float4 A = src[jj].a;
         const float4 B = src[jj].b;
+        const uint64_t sx = f2pack(A.x, A.y), sz = f2pack(A.z, A.w), sg = f2pack(B.x, B.y);
 #pragma unroll
-        for (int r = 0; r < WR; ++r) {
-            const float dx = tx[r] - A.x;
-            const float dz = tz[r] - A.z;
-            const float r2 = fmaf(dx, dx, dz * dz);
-            float K = rcp_approx(r2);
-            if (r2 < B.z) K = core_kernel(r2, B.w, K);
-            const float g = K * B.x;
-            nu[r] = fmaf(g, dz, nu[r]);
-            w[r] = fmaf(g, dx, w[r]);
+        for (int q = 0; q < WP; ++q) {
+            const uint64_t dx = f2sub(tx2[q], sx);
+            const uint64_t dz = f2sub(tz2[q], sz);
+            const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
+            const float ra = f2lo(r2), rb = f2hi(r2);
+            float ka = rcp_approx(ra), kb = rcp_approx(rb);
+            if (ra < B.z) ka = core_kernel(ra, B.w, ka);
+            if (rb < B.z) kb = core_kernel(rb, B.w, kb);
+            const uint64_t g = f2mul(f2pack(ka, kb), sg);
+            nu2[q] = f2fma(g, dz, nu2[q]);
+            w2[q] = f2fma(g, dx, w2[q]);
         }
-    }
-#pragma unroll
-    for (int q = 0; q < WP; ++q) {
-        nu2[q] = f2pack(nu[2 * q], nu[2 * q + 1]);
-        w2[q] = f2pack(w[2 * q], w[2 * q + 1]);
     }
 }
 
