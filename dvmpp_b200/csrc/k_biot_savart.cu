@@ -10,10 +10,12 @@
 // 1/sigma^2) and split into 256-blob tiles with bounding boxes.  A work item is
 // (simulation, 256 or 128 sorted targets, one source chunk); every warp pulls
 // items from an atomic counter on its own and stages 256 sources at a time in
-// its slice of shared memory.  Per staged tile the warp checks once whether any
-// of its pairs can fall inside the 10 sigma^2 core: far tiles (almost all) run
-// packed FP32x2 arithmetic with one MUFU reciprocal per pair and no test; near
-// tiles run the exact test with expm1 and the r -> 0 core limit.  Coordinates
+// its slice of shared memory.  Per staged tile the warp checks once, from the
+// boxes of its 256-target block and of the tile, whether any pair can fall
+// inside the 10 sigma^2 core: far tiles (almost all) run packed FP32x2
+// arithmetic with one MUFU reciprocal per pair and no test; near tiles run the
+// same packed arithmetic plus the exact per-pair test with expm1 and the
+// r -> 0 core limit.  Coordinates
 // are FP32 offsets from the first target of the enclosing 256-target block,
 // sums are FP32 within a stage and Kahan-compensated across stages, and chunk
 // partials are combined in FP64 in chunk order: deterministic, and independent
