@@ -992,9 +992,10 @@ int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const 
     if (e == cudaSuccess) e = pool_alloc(c, reinterpret_cast<void**>(&scratch), qr_bytes);
     if (e == cudaSuccess) {
         influence_matrix(xp, zp, xc, zc, ds, th, np, scratch, A, c->stream);
-        pseudo_inverse(A, np, P, scratch, c->stream);
-        g_launches += 2 + 1 + 2 * (uint64_t)np + 1;
-        e = cudaStreamSynchronize(c->stream);
+        e = pseudo_inverse(A, np, P, scratch, c->stream);
+        g_launches += 2 + 1 + 1 + 1 + 1;
+        const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess) e = e2;
     }
     pool_free(c, scratch);
     InstState st0;

@@ -254,7 +254,7 @@ void influence_matrix(const double* xp, const double* zp, const double* xc, cons
                       const double* ds, const double* theta, int np, double* pq_scratch,
                       double* A, cudaStream_t s);
 // Householder QR of A ((np+1) x np, row-major) and P = R^-1 Q^T (np x (np+1)).
-void pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s);
+cudaError_t pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s);
 size_t pseudo_inverse_work_doubles(int np);
 
 }  // namespace dvmk

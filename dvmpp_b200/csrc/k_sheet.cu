@@ -17,11 +17,14 @@
 // O(np^3) work per step.
 #include <cfloat>
 
+#include <cooperative_groups.h>
+
 #include "dvm_device.cuh"
 #include "dvm_internal.h"
 
 namespace dvmk {
 namespace {
+namespace cg = cooperative_groups;
 
 // ---- influence matrix -------------------------------------------------------
 __global__ void k_pq(const double* __restrict__ xp, const double* __restrict__ zp,
@@ -70,61 +73,254 @@ __global__ void k_assemble_A(const double* __restrict__ p, const double* __restr
     A[(size_t)i * np + j] = dmul(-kRpi2, dadd(p[(size_t)i * np + j], q[(size_t)i * np + jm]));
 }
 
-// ---- Householder QR of [A | I] (column-major, m = np+1 rows) -----------------
+// ---- Householder QR of A (column-major, m = np+1 rows) ------------------------
+// M holds [A | Q^T]: columns 0..np-1 are A (overwritten by R on and above the
+// diagonal and by the reflectors' tails below it), columns np..np+m-1 receive
+// Q^T.  The factorisation is one cooperative launch with one grid barrier per
+// column (it was two launches per column); Q^T is then formed by applying the
+// stored reflectors to the identity, one warp per column, in one more launch.
 __global__ void k_load_aug(const double* __restrict__ A, int np, double* __restrict__ M) {
-    const int m = np + 1, cols = np + m;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)m * cols;
+    const int m = np + 1;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)m * np;
          t += (size_t)gridDim.x * blockDim.x) {
         const int c = (int)(t / m), r = (int)(t % m);
-        M[t] = (c < np) ? A[(size_t)r * np + c] : (r == c - np ? 1.0 : 0.0);
+        M[t] = A[(size_t)r * np + c];
     }
 }
 
-__global__ void k_house(double* __restrict__ M, int np, int k, double* __restrict__ v,
-                        double* __restrict__ tau) {
-    const int m = np + 1;
-    __shared__ double s_red[32];
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Householder reflector of column k (one warp): H = I - tau v v^T maps
+// col[k..m) to (alpha, 0, ...), alpha = -sign(x0) |col[k..m)|, v = (x0 - alpha,
+// col[k+1..m)).  Writes v to vout (zeros above row k), v0 and tau to v0s[k],
+// taus[k], and alpha to col[k]; rows below k keep v's tail.
+__device__ __forceinline__ void house_col(double* __restrict__ M, int m, int k,
+                                          double* __restrict__ vout, double* __restrict__ v0s,
+                                          double* __restrict__ taus, int lane) {
     double* col = M + (size_t)k * m;
     double acc = 0.0;
-    for (int i = k + threadIdx.x; i < m; i += blockDim.x) acc = fma(col[i], col[i], acc);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double nrm2 = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) nrm2 += s_red[q];
-        const double x0 = col[k];
-        const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
-        const double v0 = x0 - alpha;
-        const double vn2 = nrm2 - x0 * x0 + v0 * v0;
-        s_red[0] = alpha;
-        s_red[1] = v0;
-        *tau = (vn2 > 0.0) ? 2.0 / vn2 : 0.0;
+    for (int i = k + lane; i < m; i += 32) acc = fma(col[i], col[i], acc);
+    const double nrm2 = warp_sum(acc);
+    const double x0 = col[k];
+    const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
+    const double v0 = x0 - alpha;
+    const double vn2 = nrm2 - x0 * x0 + v0 * v0;
+    for (int i = lane; i < m; i += 32) vout[i] = (i < k) ? 0.0 : (i == k ? v0 : col[i]);
+    __syncwarp();
+    if (lane == 0) {
+        col[k] = alpha;
+        v0s[k] = v0;
+        taus[k] = (vn2 > 0.0) ? 2.0 / vn2 : 0.0;
     }
-    __syncthreads();
-    const double alpha = s_red[0], v0 = s_red[1];
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        if (i < k) v[i] = 0.0;
-        else if (i == k) v[i] = v0;
-        else v[i] = col[i];
-    }
-    __syncthreads();
-    for (int i = k + threadIdx.x; i < m; i += blockDim.x) col[i] = (i == k) ? alpha : 0.0;
 }
 
-// Apply H = I - tau v v^T to columns k+1 .. np+m-1, one warp per column.
-__global__ void k_house_apply(double* __restrict__ M, int np, int k, const double* __restrict__ v,
-                              const double* __restrict__ tau) {
+// Cooperative launch (all blocks resident; grid.sync is the only wait).  Step
+// k: every warp applies H_k to its columns c > k; the warp holding column k+1
+// then forms reflector k+1 from it (double-buffered v), so each column costs
+// one grid barrier.
+__global__ void __launch_bounds__(256) k_qr_coop(double* __restrict__ M, int np,
+                                                 double* __restrict__ vbuf,
+                                                 double* __restrict__ v0s,
+                                                 double* __restrict__ taus) {
+    cg::grid_group grid = cg::this_grid();
+    const int m = np + 1;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int nw = (int)((gridDim.x * blockDim.x) >> 5);
+    if (gw == 0) house_col(M, m, 0, vbuf, v0s, taus, lane);
+    grid.sync();
+    for (int k = 0; k + 1 < np; ++k) {
+        const double* v = vbuf + (size_t)(k & 1) * m;
+        const double tau = taus[k];
+        for (int c = k + 1 + gw; c < np; c += nw) {
+            double* col = M + (size_t)c * m;
+            double acc = 0.0;
+            for (int i = k + lane; i < m; i += 32) acc = fma(v[i], col[i], acc);
+            const double f = warp_sum(acc) * tau;
+            for (int i = k + lane; i < m; i += 32) col[i] = fma(-f, v[i], col[i]);
+            if (c == k + 1) {
+                __syncwarp();
+                house_col(M, m, k + 1, vbuf + (size_t)((k + 1) & 1) * m, v0s, taus, lane);
+            }
+        }
+        grid.sync();
+    }
+}
+
+// Column c of Q^T = H_{np-1} ... H_0 e_c, one warp per column, the vector in
+// registers (CH = ceil(m / 32) values per lane); written to column np + c of M.
+template <int CH>
+__global__ void __launch_bounds__(128) k_form_qt(double* __restrict__ M, int np,
+                                                 const double* __restrict__ v0s,
+                                                 const double* __restrict__ taus) {
+    const int m = np + 1;
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (c >= m) return;
+    double x[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) x[t] = (lane + 32 * t == c) ? 1.0 : 0.0;
+    for (int k = 0; k < np; ++k) {
+        const double* vk = M + (size_t)k * m;  // tail below row k; v0s[k] at row k
+        const double v0 = v0s[k];
+        double acc = 0.0;
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const int i = lane + 32 * t;
+            if (i >= k && i < m) acc = fma(i == k ? v0 : vk[i], x[t], acc);
+        }
+        const double f = warp_sum(acc) * taus[k];
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const int i = lane + 32 * t;
+            if (i >= k && i < m) x[t] = fma(-f, i == k ? v0 : vk[i], x[t]);
+        }
+    }
+    double* out = M + (size_t)(np + c) * m;
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) out[i] = x[t];
+    }
+}
+
+// Reflector k of a column held in registers (CH values per lane, rows >= k
+// used): writes v to vout, v0 and tau to v0s[k], taus[k], and alpha into the
+// column.  Selects rather than branches keep x in registers.
+template <int CH>
+__device__ __forceinline__ void house_reg(double (&x)[CH], int m, int k,
+                                          double* __restrict__ vout, double* __restrict__ v0s,
+                                          double* __restrict__ taus, int lane) {
+    double acc = 0.0, xk = 0.0;
+    const int tk = k >> 5;
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int i = lane + 32 * t;
+        acc = (i >= k && i < m) ? fma(x[t], x[t], acc) : acc;
+        xk = (t == tk) ? x[t] : xk;
+    }
+    const double nrm2 = warp_sum(acc);
+    const double x0 = __shfl_sync(0xffffffffu, xk, k & 31);
+    const double alpha = (x0 >= 0.0) ? -sqrt(nrm2) : sqrt(nrm2);
+    const double v0 = x0 - alpha;
+    const double vn2 = nrm2 - x0 * x0 + v0 * v0;
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int i = lane + 32 * t;
+        if (i < m) vout[i] = (i < k) ? 0.0 : (i == k ? v0 : x[t]);
+        x[t] = (i == k) ? alpha : x[t];
+    }
+    if (lane == 0) {
+        v0s[k] = v0;
+        taus[k] = (vn2 > 0.0) ? 2.0 / vn2 : 0.0;
+    }
+}
+
+// Register-resident variant for m <= 32 CH: one warp owns one column of the
+// augmented [A | I] for the whole factorisation (CH values per lane), so a step
+// reads only the reflector from memory.  Step k: every warp with a column
+// c > k applies H_k; the warp owning column k+1 then forms reflector k+1 from
+// its registers (double-buffered v).  The identity columns become Q^T in
+// place.  At the end each warp stores its column of M.
+template <int CH>
+__global__ void __launch_bounds__(256, 2) k_qr_reg(double* __restrict__ M, int np,
+                                                double* __restrict__ vbuf,
+                                                double* __restrict__ v0s,
+                                                double* __restrict__ taus) {
+    cg::grid_group grid = cg::this_grid();
     const int m = np + 1, cols = np + m;
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int c = k + 1 + warp;
-    if (c >= cols) return;
-    double* col = M + (size_t)c * m;
-    double acc = 0.0;
-    for (int i = k + lane; i < m; i += 32) acc = fma(v[i], col[i], acc);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    const double f = acc * (*tau);
-    for (int i = k + lane; i < m; i += 32) col[i] = fma(-f, v[i], col[i]);
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const bool own = c < cols;
+    double x[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int i = lane + 32 * t;
+        const bool in = own && i < m;
+        x[t] = (in && c < np) ? M[(size_t)c * m + i] : ((in && i == c - np) ? 1.0 : 0.0);
+    }
+    if (c == 0) house_reg<CH>(x, m, 0, vbuf, v0s, taus, lane);
+    grid.sync();
+    for (int k = 0; k < np; ++k) {
+        if (own && c > k) {
+            const double* v = vbuf + (size_t)(k & 1) * m;  // zero above row k
+            double acc = 0.0;
+#pragma unroll
+            for (int t = 0; t < CH; ++t) {
+                const int i = lane + 32 * t;
+                acc = (i < m) ? fma(v[i], x[t], acc) : acc;
+            }
+            const double f = warp_sum(acc) * taus[k];
+#pragma unroll
+            for (int t = 0; t < CH; ++t) {  // second read of v hits L1
+                const int i = lane + 32 * t;
+                x[t] = (i < m) ? fma(-f, v[i], x[t]) : x[t];
+            }
+            if (c == k + 1 && k + 1 < np)
+                house_reg<CH>(x, m, k + 1, vbuf + (size_t)((k + 1) & 1) * m, v0s, taus, lane);
+        }
+        if (k + 1 < np) grid.sync();
+    }
+    if (own) {
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const int i = lane + 32 * t;
+            if (i < m) M[(size_t)c * m + i] = x[t];
+        }
+    }
+}
+
+// P[:, c] = R^-1 (Q^T)[0:np, c] with the right-hand side in registers (one warp
+// per column c, CH values per lane) and R's next column prefetched while the
+// current one is applied.
+template <int CH>
+__global__ void __launch_bounds__(256) k_backsub_reg(const double* __restrict__ M, int np,
+                                                     double* __restrict__ P) {
+    const int m = np + 1;
+    const int lane = threadIdx.x & 31;
+    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (c >= m) return;
+    const double* qt = M + (size_t)(np + c) * m;
+    double y[CH], rc[CH];
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int j = lane + 32 * t;
+        y[t] = j < np ? qt[j] : 0.0;
+        rc[t] = j < np ? M[(size_t)(np - 1) * m + j] : 0.0;  // column np-1 of R
+    }
+    for (int i = np - 1; i >= 0; --i) {
+        double rn[CH];
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {  // prefetch column i-1
+            const int j = lane + 32 * t;
+            rn[t] = (i > 0 && j < i) ? M[(size_t)(i - 1) * m + j] : 0.0;
+        }
+        // (selects rather than branches keep the arrays in registers)
+        double yi = 0.0, rii = 0.0;
+        const int ti = i >> 5;
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            yi = (t == ti) ? y[t] : yi;
+            rii = (t == ti) ? rc[t] : rii;
+        }
+        yi = __shfl_sync(0xffffffffu, yi, i & 31);
+        rii = __shfl_sync(0xffffffffu, rii, i & 31);
+        const double xi = yi / rii;
+#pragma unroll
+        for (int t = 0; t < CH; ++t) {
+            const int j = lane + 32 * t;
+            y[t] = (j < i) ? fma(-rc[t], xi, y[t]) : (j == i ? xi : y[t]);
+            rc[t] = rn[t];
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < CH; ++t) {
+        const int j = lane + 32 * t;
+        if (j < np) P[(size_t)j * m + c] = y[t];
+    }
 }
 
 // P[:, c] = R^-1 (Q^T)[0:np, c] for every column c of Q^T; one warp per column,
@@ -461,24 +657,54 @@ void influence_matrix(const double* xp, const double* zp, const double* xc, cons
 
 size_t pseudo_inverse_work_doubles(int np) {
     const size_t m = (size_t)np + 1;
-    return m * (np + m) + m + 8;
+    return m * (np + m) + 2 * m + 2 * (size_t)np + 8;
 }
 
-void pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s) {
+cudaError_t pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s) {
     const int m = np + 1, cols = np + m;
     double* M = work;
-    double* v = M + (size_t)m * cols;
-    double* tau = v + m;
+    double* vbuf = M + (size_t)m * cols;
+    double* v0s = vbuf + 2 * (size_t)m;
+    double* taus = v0s + np;
     k_load_aug<<<256, 256, 0, s>>>(A, np, M);
-    for (int k = 0; k < np; ++k) {
-        k_house<<<1, 256, 0, s>>>(M, np, k, v, tau);
-        const int ncols = cols - (k + 1);
-        const int threads = 256, wpb = threads / 32;
-        k_house_apply<<<(ncols + wpb - 1) / wpb, threads, 0, s>>>(M, np, k, v, tau);
-    }
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // Register-resident path: one warp per column of [A | I], all resident.
+    auto reg_path = [&](auto kqr, auto kbs) -> int {
+        int per = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kqr, 256, 0);
+        const int blocks = (cols + 7) / 8;
+        if (blocks > per * sms) return 0;  // not co-resident: use the general path
+        void* args[] = {&M, &np, &vbuf, &v0s, &taus};
+        cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kqr),
+                                                    dim3(blocks), dim3(256), args, 0, s);
+        if (e != cudaSuccess) return -1;
+        kbs<<<(m + 7) / 8, 256, 0, s>>>(M, np, P);
+        return 1;
+    };
+    int done = 0;
+    if (m <= 32 * 9) done = reg_path(k_qr_reg<9>, k_backsub_reg<9>);
+    else if (m <= 32 * 17) done = reg_path(k_qr_reg<17>, k_backsub_reg<17>);
+    else if (m <= 32 * 33) done = reg_path(k_qr_reg<33>, k_backsub_reg<33>);
+    if (done < 0) return cudaGetLastError();
+    if (done > 0) return cudaGetLastError();
+    // General path: one warp per column of A (columns in memory), then Q^T
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qr_coop, 256, 0);
+    const int blocks = std::max(1, std::min((np + 7) / 8, std::max(1, per_sm) * sms));
+    void* args[] = {&M, &np, &vbuf, &v0s, &taus};
+    cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_qr_coop),
+                                                dim3(blocks), dim3(256), args, 0, s);
+    if (e != cudaSuccess) return e;
+    const int g = (m + 3) / 4;  // 4 warps (columns) per block
+    if (m <= 32 * 9) k_form_qt<9><<<g, 128, 0, s>>>(M, np, v0s, taus);
+    else if (m <= 32 * 17) k_form_qt<17><<<g, 128, 0, s>>>(M, np, v0s, taus);
+    else if (m <= 32 * 33) k_form_qt<33><<<g, 128, 0, s>>>(M, np, v0s, taus);
+    else k_form_qt<65><<<g, 128, 0, s>>>(M, np, v0s, taus);  // np <= 2048
     // warps per block such that the per-warp right-hand sides fit 48 KB of shared memory
     const int wpb = std::max(1, std::min(4, (int)(48 * 1024 / (sizeof(double) * np))));
     k_backsub<<<(m + wpb - 1) / wpb, wpb * 32, sizeof(double) * np * wpb, s>>>(M, np, P);
+    return cudaGetLastError();
 }
 
 void sheet_solve(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,

@@ -97,6 +97,20 @@ def test_empty_blob_solve(ctx, port):
     s.close()
 
 
+@pytest.mark.parametrize("npanels", [40, 300, 700, 1100])
+def test_pseudo_inverse_every_kernel_path(ctx, npanels):
+    """The once-per-body factorisation has a register-resident path per column
+    length (m = np + 1 <= 288, 544, 1056) and a general path above that; each
+    must give the least-squares gamma of the influence matrix it built."""
+    bx, bz = W.ellipse(npanels, incidence_deg=20.0)
+    s = ctx.sim(params(capacity=4096, ux=1.0), bx, bz)
+    s.phase(N.PHASE_SOLVE)
+    A, b = s.influence(), s.rhs()
+    ref = np.linalg.lstsq(A, b, rcond=None)[0]
+    assert close(s.gamma(), ref, 1e-10), npanels
+    s.close()
+
+
 def test_diffusion_inject_matches(ctx, port):
     bx, bz = W.circle(64)
     p = params(nu=1e-3, dt=0.01)
