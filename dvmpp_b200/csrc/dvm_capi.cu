@@ -769,6 +769,26 @@ int dvm_ctx_reserve(dvm_ctx* c, uint64_t total_capacity, int max_sims, int max_p
                             max_sims, with_delete != 0);
 }
 
+int dvm_ctx_pool_reserve(dvm_ctx* c, uint64_t bytes) {
+    if (!c) return fail(DVM_ERR_ARG, "null context");
+    if (bytes == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    uint64_t held = 0;
+    CK(cudaMemPoolGetAttribute(c->mempool, cudaMemPoolAttrReservedMemCurrent, &held));
+    if (held >= bytes) return DVM_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, c->mempool, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DVM_ERR_OOM, std::string("pool reserve: ") + cudaGetErrorString(e));
+    }
+    e = cudaFreeAsync(p, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return fail(DVM_ERR_CUDA, std::string("pool reserve: ") + cudaGetErrorString(e));
+    return DVM_OK;
+}
+
 int dvm_ctx_workspace_bytes(dvm_ctx* c, uint64_t* bytes) {
     if (!c || !bytes) return fail(DVM_ERR_ARG, "null argument");
     *bytes = c->ws_bytes;

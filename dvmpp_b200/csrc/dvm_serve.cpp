@@ -146,6 +146,21 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
         uint64_t used = 0, total = 0;
         dvm_ctx_memory(s->ctx, &used, &total);
         s->budget = std::min<uint64_t>(s->budget, total > used ? total - used : 0);
+        // Map the pool once for the cap_active largest slabs (and the largest
+        // set-up scratch), within the budget, so admissions do not grow it.
+        std::vector<uint64_t> slabs;
+        uint64_t scratch = 0;
+        for (auto& r : s->reqs) {
+            slabs.push_back(r.bytes);
+            const uint64_t np = r.bx.size() - 1;  // influence + factorisation scratch
+            scratch = std::max<uint64_t>(
+                scratch, 8 * (2 * np * np + dvmk::pseudo_inverse_work_doubles((int)np)));
+        }
+        std::sort(slabs.rbegin(), slabs.rend());
+        uint64_t want = scratch;
+        for (size_t i = 0; i < slabs.size() && (int)i < cap_active; ++i) want += slabs[i];
+        // (an unreserved pool still works, only slower to admit)
+        (void)dvm_ctx_pool_reserve(s->ctx, std::min<uint64_t>(want, s->budget));
     }
     std::vector<size_t> order(s->reqs.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;

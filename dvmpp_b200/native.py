@@ -166,6 +166,10 @@ class Context:
         _check(self.lib.dvm_ctx_memory(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def pool_reserve(self, nbytes: int):
+        """Map the stream-ordered pool for simulation slabs up to nbytes once."""
+        _check(self.lib.dvm_ctx_pool_reserve(self.h, int(nbytes)))
+
     def device_info(self):
         s, ma, mi = C.c_int(), C.c_int(), C.c_int()
         _check(self.lib.dvm_ctx_device_info(self.h, C.byref(s), C.byref(ma), C.byref(mi)))
@@ -609,6 +613,7 @@ SIGNATURES.update({
     "dvm_sim_clear_uniforms": (C.c_int, [C.c_void_p]),
     "dvm_sim_pending_uniforms": (C.c_int, [C.c_void_p, _dp, C.c_uint64, C.POINTER(C.c_uint64)]),
     "dvm_ctx_workspace_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "dvm_ctx_pool_reserve": (C.c_int, [C.c_void_p, C.c_uint64]),
     "dvm_server_create": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "dvm_server_destroy": (C.c_int, [C.c_void_p]),
     "dvm_server_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),

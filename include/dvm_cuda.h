@@ -147,6 +147,12 @@ int dvm_ctx_launch_count(dvm_ctx* ctx, uint64_t* launches);
 int dvm_ctx_reserve(dvm_ctx* ctx, uint64_t total_capacity, int max_sims, int max_panels,
                     int with_delete);
 int dvm_ctx_workspace_bytes(dvm_ctx* ctx, uint64_t* bytes);
+/* Grow the context's stream-ordered memory pool (simulation slabs and set-up
+ * scratch come from it) to hold at least `bytes`, once, so that admissions
+ * carve their slabs from memory already mapped instead of growing the pool
+ * one simulation at a time.  The memory stays with the pool until the ctx is
+ * destroyed; it does not count against the simulations' HBM budget. */
+int dvm_ctx_pool_reserve(dvm_ctx* ctx, uint64_t bytes);
 /* Timing markers: dvm_ctx_mark records CUDA event `slot` (0..15) on the ctx
  * stream; dvm_ctx_elapsed synchronises and returns the device time between
  * two recorded markers. */
