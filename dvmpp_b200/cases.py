@@ -15,6 +15,11 @@ precision: ellipse (0.5, 0.25) at 20 degrees, 1024 panels (a 1025 x 1024
 influence matrix), a 2^19-blob wake, RK3 dt = 0.002; the FP32-compensated run
 (FP64 QR, FP64 refinement and Kelvin row) against an all-FP64 run.
 
+    python -m dvmpp_b200.cases sheet [--n 131072] [--panels 1024] [--reps 3]
+
+sheet: the FP32 sheet-on-blob velocity alone (ellipse at 20 degrees, wake of
+n blobs); prints its CUDA-event time, pairs/s and FP32 fraction (67 flop/pair).
+
     python -m dvmpp_b200.cases serve [--requests 100] [--serial] [--realtime]
 
 serve: the continuous-batching server on Poisson arrivals (seed 7, 20 req/s).
@@ -215,6 +220,36 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
             "per_step": rows}
 
 
+def run_sheet(n: int, npanels: int, reps: int, seed: int = 2):
+    """Sheet-on-blob velocity alone: an ellipse (0.5, 0.25) at 20 degrees with
+    npanels panels, an n-blob wake (the N-body distribution, core size of this
+    body), FP32 instance; blob velocities and the panel strengths are computed
+    once, then the sheet-on-blob phase runs reps times (the first untimed)."""
+    ctx = N.Context(0)
+    sms, _, _ = ctx.device_info()
+    bx, bz = W.ellipse(npanels, incidence_deg=20.0)
+    x, z, g, s = W.wake(n, seed, W.core_size(bx, bz))
+    sim = ctx.sim(N.Params(capacity=n, precision=N.F32, rng=N.RNG_PHILOX, ux=1.0), bx, bz)
+    sim.set_blobs(x, z, g, s)
+    sim.phase(N.PHASE_BIOTSAVART)
+    sim.phase(N.PHASE_SOLVE)
+    sim.phase(N.PHASE_SHEETBC)  # warm-up
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    for _ in range(reps):
+        sim.phase(N.PHASE_SHEETBC)
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    ms = prof["sheetvel"][0] / max(prof["sheetvel"][1], 1)
+    pairs = n * npanels
+    tf = 67.0 * pairs / (ms / 1e3) / 1e12
+    sim.close()
+    ctx.close()
+    return {"workload": "sheet", "n": n, "panels": npanels, "pairs": pairs, "kernel_ms": ms,
+            "gpairs_per_s": pairs / (ms / 1e3) / 1e9, "tflops_67_per_pair": tf,
+            "fp32_peak_frac": tf / _fp32_peak_tflops(sms)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -237,6 +272,10 @@ def main(argv=None):
     sv.add_argument("--no-sync", action="store_true")
     sv.add_argument("--autotune", action="store_true",
                     help="tune the pair kernel once per new batch-shape class")
+    sh = sub.add_parser("sheet")
+    sh.add_argument("--n", type=int, default=1 << 17)
+    sh.add_argument("--panels", type=int, default=1024)
+    sh.add_argument("--reps", type=int, default=3)
     pr = sub.add_parser("precision")
     pr.add_argument("--steps", type=int, default=20)
     pr.add_argument("--n-wake", type=int, default=1 << 19)
@@ -249,6 +288,8 @@ def main(argv=None):
         print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
                                      a.max_active, a.budget_gb, a.realtime, a.serial,
                                      not a.no_graph, not a.no_sync, a.autotune)))
+    if a.cmd == "sheet":
+        print(json.dumps(run_sheet(a.n, a.panels, a.reps)))
     if a.cmd == "nbody":
         precs = {"f32": [N.F32], "f64": [N.F64], "both": [N.F32, N.F64]}[a.prec]
         print(json.dumps(run_nbody(a.n, precs, a.reps, a.seed)))
