@@ -75,10 +75,14 @@ __global__ void k_assemble_A(const double* __restrict__ p, const double* __restr
 
 // ---- Householder QR of A (column-major, m = np+1 rows) ------------------------
 // M holds [A | Q^T]: columns 0..np-1 are A (overwritten by R on and above the
-// diagonal and by the reflectors' tails below it), columns np..np+m-1 receive
-// Q^T.  The factorisation is one cooperative launch with one grid barrier per
-// column (it was two launches per column); Q^T is then formed by applying the
-// stored reflectors to the identity, one warp per column, in one more launch.
+// diagonal), columns np..np+m-1 receive Q^T.  Both paths are one cooperative
+// launch with one grid barrier per Householder step (a chain of np dependent
+// steps; separate launches per step cost ~2.5 us each).  For m <= 1056 each
+// warp keeps one column of [A | I] in registers and the identity columns turn
+// into Q^T in place (k_qr_reg); above that the columns of A stay in memory,
+// their reflectors' tails are kept below the diagonal, and Q^T is formed
+// afterwards by applying the stored reflectors to the identity (k_qr_coop,
+// k_form_qt).
 __global__ void k_load_aug(const double* __restrict__ A, int np, double* __restrict__ M) {
     const int m = np + 1;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)m * np;
