@@ -19,6 +19,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
+// One MUFU base-2 exponential (relative error below 2^-22 on B200-class parts).
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11): 10 rounds of the
 // 4x32 bijection with multipliers 0xD2511F53 / 0xCD9E8D57 and Weyl key

@@ -267,20 +267,43 @@ __device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
     }
 }
 
-// Core kernel (1 - exp(-r2/sigma^2)) / r2 in FP32.  expm1 keeps close pairs
-// accurate; below FLT_MIN the r -> 0 limit 1/sigma^2 is used.  That limit
-// covers the self pair (dx = dz = 0, so its contribution is exactly zero, as
-// the reference's i != j skip gives) and distinct blobs closer than FP32 can
-// resolve (nascent blobs of one panel can be), where the FP64 reference is
-// finite too.
+// Core kernel (1 - exp(-r2/sigma^2)) / r2 in FP32, written as rs phi(t) with
+// t = r2 rs, rs = 1/sigma^2 and phi(t) = (1 - e^-t) / t.  For t < 1/2 phi is
+// its Taylor series sum_k (-t)^k / (k+1)! to degree 8 (truncation below 6e-10
+// relative, and phi(0) = 1 gives the r -> 0 limit 1/sigma^2: the self pair
+// then contributes exactly zero, as the reference's i != j skip gives, and
+// distinct blobs closer than FP32 resolves stay finite, as the FP64 reference
+// is).  For t >= 1/2 it is (1 - e) / r2 with e = 2^(-t log2 e) from one MUFU
+// ex2; 1 - e >= 0.39 there, so the ex2 error stays below 4e-7 relative.
 __device__ __forceinline__ float core_kernel(float r2, float rs, float rcp_r2) {
+    const float t = r2 * rs;
+    float p = 1.0f / 362880.0f;
+    p = fmaf(p, t, -1.0f / 40320.0f);
+    p = fmaf(p, t, 1.0f / 5040.0f);
+    p = fmaf(p, t, -1.0f / 720.0f);
+    p = fmaf(p, t, 1.0f / 120.0f);
+    p = fmaf(p, t, -1.0f / 24.0f);
+    p = fmaf(p, t, 1.0f / 6.0f);
+    p = fmaf(p, t, -0.5f);
+    p = fmaf(p, t, 1.0f);
+    const float e = ex2_approx(-t * 1.44269504088896341f);
+    return t < 0.5f ? rs * p : (1.0f - e) * rcp_r2;
+}
+
+// The same core kernel through expm1f (about 1 ulp): the blob-on-collocation
+// right-hand side keeps it, since that sum is a small residual of nearly
+// cancelling terms.  Below FLT_MIN the r -> 0 limit 1/sigma^2 is used.
+__device__ __forceinline__ float core_kernel_expm1(float r2, float rs, float rcp_r2) {
     const float e = expm1f(-r2 * rs);
     return r2 > 1e-30f ? -e * rcp_r2 : rs;
 }
 
 // Near pairs: the reference's exact test per pair.  The shared arithmetic is
 // packed like the far path (each half rounds like the scalar instruction, so a
-// pair gets the same bits on either path); only the core kernel runs per pair.
+// pair outside the core gets the same bits on either path); the core kernel
+// runs for both halves of a packed pair, branch-free, whenever any lane of the
+// warp has a pair inside the core, and a select keeps it only for those pairs,
+// so a pair's value does not depend on its neighbours in the warp.
 template <int WP>
 __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
                                            const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
@@ -297,8 +320,12 @@ __device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
             const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
             const float ra = f2lo(r2), rb = f2hi(r2);
             float ka = rcp_approx(ra), kb = rcp_approx(rb);
-            if (ra < B.z) ka = core_kernel(ra, B.w, ka);
-            if (rb < B.z) kb = core_kernel(rb, B.w, kb);
+            const bool ca = ra < B.z, cb = rb < B.z;
+            if (__any_sync(0xffffffffu, ca || cb)) {
+                const float qa = core_kernel(ra, B.w, ka), qb = core_kernel(rb, B.w, kb);
+                ka = ca ? qa : ka;
+                kb = cb ? qb : kb;
+            }
             const uint64_t g = f2mul(f2pack(ka, kb), sg);
             nu2[q] = f2fma(g, dz, nu2[q]);
             w2[q] = f2fma(g, dx, w2[q]);
@@ -614,7 +641,7 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
                     const float r2 = fmaf(dx, dx, dz * dz);
                     if (J.skip_close && !(r2 > 1e-15f)) continue;
                     float K = rcp_approx(r2);
-                    if (r2 < s_thrf[jj]) K = core_kernel(r2, s_rsf[jj], K);
+                    if (r2 < s_thrf[jj]) K = core_kernel_expm1(r2, s_rsf[jj], K);
                     const float g = K * s_cf[jj];
                     kahan(su, cu, -g * dz);
                     kahan(sw, cw, g * dx);
