@@ -14,8 +14,9 @@
 // boxes of its 256-target block and of the tile, whether any pair can fall
 // inside the 10 sigma^2 core: far tiles (almost all) run packed FP32x2
 // arithmetic with one MUFU reciprocal per pair and no test; near tiles run the
-// same packed arithmetic plus the exact per-pair test with expm1 and the
-// r -> 0 core limit.  Coordinates
+// same packed arithmetic plus the exact per-pair test, the core kernel
+// evaluated as (1/sigma^2) phi(r^2/sigma^2) with the r -> 0 limit built in
+// (core_kernel).  Coordinates
 // are FP32 offsets from the first target of the enclosing 256-target block,
 // sums are FP32 within a stage and Kahan-compensated across stages, and chunk
 // partials are combined in FP64 in chunk order: deterministic, and independent
