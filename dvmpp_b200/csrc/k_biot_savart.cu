@@ -231,14 +231,34 @@ __device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c) {
     return d;
 }
 
-// Staged source: A = (x, x, z, z), B = (Gamma, Gamma, 10 sigma^2, 1/sigma^2), so
-// the far loop loads the duplicated pairs straight into 64-bit registers.
-struct StagedSrc {
-    float4 a;
-    float4 b;
+// A warp's staged source tile: pos2[i] = (x, z) of sources 2i and 2i+1 (FP32
+// offsets), gam2[i] = (Gamma, Gamma) of both, core[j] = (10 sigma^2,
+// 1/sigma^2).  The loops read two sources with two 16-byte loads and duplicate
+// x and z into packed register pairs themselves (half the shared-memory loads
+// of one 32-byte record per source: 0.6 % faster, same results).
+struct StagedTile {
+    float4 pos2[kBsST / 2];
+    float4 gam2[kBsST / 2];
+    float2 core[kBsST];
 };
 
-constexpr int kFarUnroll = 8;  // sources per unrolled far-loop body
+// One staged source against the warp's targets (far: no core test).
+template <int WP>
+__device__ __forceinline__ void far_pair(uint64_t sx, uint64_t sz, uint64_t sg,
+                                         const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
+                                         uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
+#pragma unroll
+    for (int q = 0; q < WP; ++q) {
+        const uint64_t dx = f2sub(tx2[q], sx);
+        const uint64_t dz = f2sub(tz2[q], sz);
+        const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
+        // one MUFU reciprocal per pair (padded sources: rcp of ~2e36, Gamma 0)
+        const uint64_t inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
+        const uint64_t g = f2mul(inv, sg);
+        nu2[q] = f2fma(g, dz, nu2[q]);
+        w2[q] = f2fma(g, dx, w2[q]);
+    }
+}
 
 // Far pairs: no core test.  Accumulates -u (so every update is one FMA) and w.
 // (Sharing one reciprocal between the two targets of a packed pair, 1/a = b/(ab),
@@ -246,25 +266,15 @@ constexpr int kFarUnroll = 8;  // sources per unrolled far-loop body
 // slower for 1/8 to 1/2 of the sources, the FMA pipe being nearly as loaded as
 // the MUFU pipe.)
 template <int WP>
-__device__ __forceinline__ void stage_far(const StagedSrc* __restrict__ src,
+__device__ __forceinline__ void stage_far(const StagedTile& __restrict__ src,
                                           const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                           uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
-#pragma unroll kFarUnroll
-    for (int jj = 0; jj < kBsST; ++jj) {
-        const float4 A = src[jj].a;
-        const float4 B = src[jj].b;
-        const uint64_t sx = f2pack(A.x, A.y), sz = f2pack(A.z, A.w), sg = f2pack(B.x, B.y);
-#pragma unroll
-        for (int q = 0; q < WP; ++q) {
-            const uint64_t dx = f2sub(tx2[q], sx);
-            const uint64_t dz = f2sub(tz2[q], sz);
-            const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
-            // one MUFU reciprocal per pair (padded sources: rcp of ~2e36, Gamma 0)
-            const uint64_t inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
-            const uint64_t g = f2mul(inv, sg);
-            nu2[q] = f2fma(g, dz, nu2[q]);
-            w2[q] = f2fma(g, dx, w2[q]);
-        }
+#pragma unroll 4  // 8 sources per unrolled body
+    for (int i = 0; i < kBsST / 2; ++i) {
+        const float4 P = src.pos2[i];
+        const float4 G = src.gam2[i];
+        far_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), tx2, tz2, nu2, w2);
+        far_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), tx2, tz2, nu2, w2);
     }
 }
 
@@ -299,6 +309,30 @@ __device__ __forceinline__ float core_kernel_expm1(float r2, float rs, float rcp
     return r2 > 1e-30f ? -e * rcp_r2 : rs;
 }
 
+// One staged source against the warp's targets with the exact core test.
+template <int WP>
+__device__ __forceinline__ void near_pair(uint64_t sx, uint64_t sz, uint64_t sg, float2 C,
+                                          const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
+                                          uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
+#pragma unroll
+    for (int q = 0; q < WP; ++q) {
+        const uint64_t dx = f2sub(tx2[q], sx);
+        const uint64_t dz = f2sub(tz2[q], sz);
+        const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
+        const float ra = f2lo(r2), rb = f2hi(r2);
+        float ka = rcp_approx(ra), kb = rcp_approx(rb);
+        const bool ca = ra < C.x, cb = rb < C.x;
+        if (__any_sync(0xffffffffu, ca || cb)) {
+            const float qa = core_kernel(ra, C.y, ka), qb = core_kernel(rb, C.y, kb);
+            ka = ca ? qa : ka;
+            kb = cb ? qb : kb;
+        }
+        const uint64_t g = f2mul(f2pack(ka, kb), sg);
+        nu2[q] = f2fma(g, dz, nu2[q]);
+        w2[q] = f2fma(g, dx, w2[q]);
+    }
+}
+
 // Near pairs: the reference's exact test per pair.  The shared arithmetic is
 // packed like the far path (each half rounds like the scalar instruction, so a
 // pair outside the core gets the same bits on either path); the core kernel
@@ -306,31 +340,16 @@ __device__ __forceinline__ float core_kernel_expm1(float r2, float rs, float rcp
 // warp has a pair inside the core, and a select keeps it only for those pairs,
 // so a pair's value does not depend on its neighbours in the warp.
 template <int WP>
-__device__ __forceinline__ void stage_near(const StagedSrc* __restrict__ src,
+__device__ __forceinline__ void stage_near(const StagedTile& __restrict__ src,
                                            const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                            uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
-#pragma unroll 2
-    for (int jj = 0; jj < kBsST; ++jj) {
-        const float4 A = src[jj].a;
-        const float4 B = src[jj].b;
-        const uint64_t sx = f2pack(A.x, A.y), sz = f2pack(A.z, A.w), sg = f2pack(B.x, B.y);
-#pragma unroll
-        for (int q = 0; q < WP; ++q) {
-            const uint64_t dx = f2sub(tx2[q], sx);
-            const uint64_t dz = f2sub(tz2[q], sz);
-            const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
-            const float ra = f2lo(r2), rb = f2hi(r2);
-            float ka = rcp_approx(ra), kb = rcp_approx(rb);
-            const bool ca = ra < B.z, cb = rb < B.z;
-            if (__any_sync(0xffffffffu, ca || cb)) {
-                const float qa = core_kernel(ra, B.w, ka), qb = core_kernel(rb, B.w, kb);
-                ka = ca ? qa : ka;
-                kb = cb ? qb : kb;
-            }
-            const uint64_t g = f2mul(f2pack(ka, kb), sg);
-            nu2[q] = f2fma(g, dz, nu2[q]);
-            w2[q] = f2fma(g, dx, w2[q]);
-        }
+#pragma unroll 1
+    for (int i = 0; i < kBsST / 2; ++i) {
+        const float4 P = src.pos2[i];
+        const float4 G = src.gam2[i];
+        const float2 C0 = src.core[2 * i], C1 = src.core[2 * i + 1];
+        near_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), C0, tx2, tz2, nu2, w2);
+        near_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), C1, tx2, tz2, nu2, w2);
     }
 }
 
@@ -348,7 +367,7 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
                const TileMeta* __restrict__ meta, double2* __restrict__ part,
                unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
-    __shared__ StagedSrc s_src[kWWarps][kBsST];
+    __shared__ StagedTile s_src[kWWarps];
     constexpr int kWP = WR / 2, kWTT = 32 * WR;
     if (threadIdx.x == 0) {
         unsigned acc = 0;
@@ -361,7 +380,9 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
     __syncthreads();
     const unsigned total = s_pre[nlist];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    StagedSrc* __restrict__ wsrc = s_src[wid];
+    StagedTile& wsrc = s_src[wid];
+    float2* __restrict__ wpos = reinterpret_cast<float2*>(wsrc.pos2);
+    float2* __restrict__ wgam = reinterpret_cast<float2*>(wsrc.gam2);
     for (;;) {
         unsigned item = 0;
         if (lane == 0) item = atomicAdd(work, 1u);
@@ -413,18 +434,17 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
 #pragma unroll
             for (int q = 0; q < kBsST / 32; ++q) {
                 const uint32_t jj = q * 32 + lane, j = s0 + jj;
-                StagedSrc v;
                 if (j < j1) {
                     const double2 p = X[j];
                     const float4 f = F[j];  // (circ, 10 sigma^2, 1/sigma^2, -)
-                    const float px = (float)(p.x - o.x), pz = (float)(p.y - o.y);
-                    v.a = make_float4(px, px, pz, pz);
-                    v.b = make_float4(f.x, f.x, f.y, f.z);
+                    wpos[jj] = make_float2((float)(p.x - o.x), (float)(p.y - o.y));
+                    wgam[jj] = make_float2(f.x, f.x);
+                    wsrc.core[jj] = make_float2(f.y, f.z);
                 } else {  // padding: far away, no circulation, never in a core
-                    v.a = make_float4(1e18f, 1e18f, 1e18f, 1e18f);
-                    v.b = make_float4(0.0f, 0.0f, -1.0f, 0.0f);
+                    wpos[jj] = make_float2(1e18f, 1e18f);
+                    wgam[jj] = make_float2(0.0f, 0.0f);
+                    wsrc.core[jj] = make_float2(-1.0f, 0.0f);
                 }
-                wsrc[jj] = v;
             }
             __syncwarp();
             const TileMeta m = meta[(e.coff + s0) / kBsST];
