@@ -151,17 +151,20 @@ def make_instances(count: int, seed: int):
     return W.batched_instances(count, seed)
 
 
-def sim_params(inst, steps_total: int, prepush_steps: int):
+def sim_params(inst, steps_total: int, prepush_steps: int, async_steps: int = 0):
+    """async_steps: room for that many per-step pushes on top of the prepushed
+    uniforms (asynchronous pushes append without compacting the stream)."""
     from dvmpp_b200 import native as N
 
     M = 3
     grow = steps_total * (M + 1) * inst["npanels"] * 2  # release counts can exceed (M+1)
     cap = inst["nblobs"] + grow
     per_step = 2 * cap + 2 * (M + 1) * inst["npanels"]
+    push_ub = 2 * (cap + 2 * (M + 1) * inst["npanels"]) + 2 * (M + 1) * inst["npanels"] + 64
     return N.Params(rho=1.0, nu=1e-3, dt=0.005, ux=1.0, uz=0.0, cutoff_exp=0.675,
                     max_numpanelvort=M, scheme=N.EULER, surface_cross=N.REFLECT,
                     rng=N.RNG_INJECT, precision=N.F32, seed=1, capacity=cap,
-                    rng_capacity=prepush_steps * per_step + 1024)
+                    rng_capacity=prepush_steps * per_step + 1024 + async_steps * push_ub)
 
 
 def pinned(n: int):
@@ -365,7 +368,7 @@ def run_ours(args, dist):
     prepush = args.warmup + args.steps + args.prof_steps + args.plain_steps + 1
     sims = []
     for inst in instances:
-        p = sim_params(inst, steps_total, prepush)
+        p = sim_params(inst, steps_total, prepush, args.e2e_steps + 1 if args.e2e_steps else 0)
         bx, bz = inst["body"]
         s = ctx.sim(p, bx, bz)
         s.set_blobs(*inst["blobs"])
@@ -453,11 +456,13 @@ def run_ours(args, dist):
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
-        # The user's loop, pipelined as an application would run it: launch
-        # step k, generate the next step's uniforms on the host while the GPU
-        # computes, read step k's blobs and loads back, push the uniforms.
-        # Uniforms are pushed for an upper bound of the next step's draws (the
-        # device consumes them in order; the surplus carries over).
+        # The user's loop, pipelined as an application would run it: while the
+        # GPU computes step k the host generates step k+1's uniforms, pushes
+        # them (copy stream) and enqueues step k+1; step k's snapshot (x, z,
+        # circ of every blob and the loads, taken on the GPU right after step k)
+        # is then copied out while step k+1 runs.  Uniforms are pushed for an
+        # upper bound of the next step's draws (the device consumes them in
+        # order; the surplus carries over).
         M = 3
         ub = [2 * (s.n_hint + 2 * (M + 1) * s.np) + 2 * (M + 1) * s.np + 64 for s in sims]
         hbuf = [[pinned(u) for u in ub] for _ in range(2)]
@@ -479,29 +484,34 @@ def run_ours(args, dist):
         dist.barrier()
         ctx.sync()
         t0 = time.perf_counter()
-        ctx.batch_push_uniforms(sims, hbuf[0], sizes)  # one wait for all simulations
+        ctx.batch_push_uniforms_async(sims, hbuf[0], sizes)
         h2d += 8 * sum(sizes)
+        ctx.step_batch(sims, 1, use_graph=True)
+        ctx.batch_get_state_async(sims)
         for step in range(args.e2e_steps):
-            ctx.step_batch(sims, 1, use_graph=True)  # asynchronous
             last = step + 1 == args.e2e_steps
             if not last:
                 sizes = generate(hbuf[(step + 1) % 2])  # overlaps the GPU step
-            # x, z, circ of every blob and the loads of every simulation, one wait
-            nprev, loads = ctx.batch_get_state(sims, out_x, out_z, out_c)
+                ctx.batch_push_uniforms_async(sims, hbuf[(step + 1) % 2], sizes)
+                h2d += 8 * sum(sizes)
+                ctx.step_batch(sims, 1, use_graph=True)  # queued behind this step
+            # this step's x, z, circ and loads; the copy overlaps the next step
+            nprev, loads = ctx.batch_wait_state(out_x, out_z, out_c)
             d2h += sum(3 * 8 * n + 4 * 8 for n in nprev)
             if not last:
-                ctx.batch_push_uniforms(sims, hbuf[(step + 1) % 2], sizes)
-                h2d += 8 * sum(sizes)
+                ctx.batch_get_state_async(sims)
         ctx.sync()
         e2e_s = dist.max(time.perf_counter() - t0)
         e2e = {"value": dist.world * args.instances * args.e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d / args.e2e_steps),
                "d2h_bytes_per_step": int(d2h / args.e2e_steps),
                "note": "per step: the step's uniforms (inject mode) pushed from pinned "
-                       "memory (the next step's are generated on the host while the GPU "
-                       "computes; the first step's before the clock starts), one batched "
-                       "step, x/z/circ of every blob and the loads read back (what "
-                       "DVMBase::write_outputs consumes); host wall clock"}
+                       "memory, one batched step, x/z/circ of every blob and the loads "
+                       "read back (what DVMBase::write_outputs consumes); pipelined: the "
+                       "next step's uniforms are generated and pushed and the next step "
+                       "enqueued while the GPU computes, and a step's state is copied "
+                       "out while the next one runs (the first step's uniforms are "
+                       "generated before the clock starts); host wall clock"}
         for s in sims:
             s.check()
 

@@ -172,6 +172,18 @@ struct dvm_ctx {
     double prof_ms[DVM_PROF_FAMILIES] = {};
     uint64_t prof_n[DVM_PROF_FAMILIES] = {};
     cudaEvent_t marks[16] = {};
+    // pipelined host loops: a copy stream for uniforms pushed and snapshots
+    // read back while the compute stream runs the neighbouring step
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t push_ev = nullptr, snap_ev = nullptr;
+    double* snap_buf = nullptr;  // pool memory: x, z, circ of every snapshotted simulation
+    uint64_t snap_doubles = 0;
+    InstState* h_state_snap = nullptr;  // pinned copy of the state table at the snapshot
+    uint64_t* h_ucount = nullptr;  // pinned staging of the uniform counts pushed asynchronously
+    cudaEvent_t ucount_ev = nullptr;  // the last upload from h_ucount
+    std::vector<int> snap_slots;
+    std::vector<uint64_t> snap_off, snap_cap;
+    bool snap_pending = false;
 };
 
 struct dvm_sim {
@@ -726,6 +738,19 @@ int dvm_ctx_destroy(dvm_ctx* c) {
     if (c->list_pool) cudaFree(c->list_pool);
     if (c->d_tune_list) cudaFree(c->d_tune_list);
     if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->snap_buf) {
+        pool_free(c, c->snap_buf);
+        cudaStreamSynchronize(c->stream);
+    }
+    if (c->push_ev) cudaEventDestroy(c->push_ev);
+    if (c->snap_ev) cudaEventDestroy(c->snap_ev);
+    if (c->h_state_snap) cudaFreeHost(c->h_state_snap);
+    if (c->h_ucount) cudaFreeHost(c->h_ucount);
+    if (c->ucount_ev) cudaEventDestroy(c->ucount_ev);
     if (c->d_table) cudaFree(c->d_table);
     if (c->d_state) cudaFree(c->d_state);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1040,6 +1065,7 @@ int dvm_sim_destroy(dvm_sim* s) {
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);  // no graph of this simulation may still run
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);  // nor a copy into it
     drop_plans_with(c, s->slot);
     c->slots[s->slot] = nullptr;
     c->in_use -= s->bytes;
@@ -1211,6 +1237,7 @@ int dvm_sim_push_uniforms(dvm_sim* s, const double* u, uint64_t n) {
     if (!s || (n && !u)) return fail(DVM_ERR_ARG, "null argument");
     if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
     cudaStream_t st = s->ctx->stream;
+    if (s->ctx->copy_stream) CK(cudaStreamSynchronize(s->ctx->copy_stream));
     uint64_t cursor = 0;
     CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -1321,6 +1348,7 @@ int dvm_batch_push_uniforms(dvm_ctx* c, dvm_sim* const* sims, int nsims, const d
     if (nsims == 0) return DVM_OK;
     std::lock_guard<std::mutex> lk(c->mu);
     CK(cudaSetDevice(c->device));
+    if (c->copy_stream) CK(cudaStreamSynchronize(c->copy_stream));  // compaction moves data
     int rc = read_states(c, sims, nsims);
     if (rc) return rc;
     const uint64_t zero = 0;
@@ -1350,6 +1378,153 @@ int dvm_batch_push_uniforms(dvm_ctx* c, dvm_sim* const* sims, int nsims, const d
         if (rc) return rc;
     }
     CK(cudaStreamSynchronize(c->stream));
+    return DVM_OK;
+}
+
+namespace {
+int ensure_async(dvm_ctx* c) {
+    if (c->copy_stream) return DVM_OK;
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->push_ev, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->snap_ev, cudaEventDisableTiming));
+    CK(cudaMallocHost(&c->h_state_snap, sizeof(InstState) * (size_t)kTableCap));
+    CK(cudaMallocHost(&c->h_ucount, sizeof(uint64_t) * (size_t)kTableCap));
+    CK(cudaEventCreateWithFlags(&c->ucount_ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->ucount_ev, c->stream));
+    return DVM_OK;
+}
+}  // namespace
+
+int dvm_batch_push_uniforms_async(dvm_ctx* c, dvm_sim* const* sims, int nsims,
+                                  const double* const* u, const uint64_t* counts) {
+    if (!c || nsims < 0 || (nsims && (!sims || !u || !counts)))
+        return fail(DVM_ERR_ARG, "bad argument");
+    if (nsims == 0) return DVM_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    for (int i = 0; i < nsims; ++i) {  // check everything before copying anything
+        dvm_sim* s = sims[i];
+        if (!s || s->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
+        if (counts[i] && !u[i]) return fail(DVM_ERR_ARG, "null uniform array");
+        if (s->h.ucount + counts[i] > s->ucap)
+            return fail(DVM_ERR_CAPACITY,
+                        "uniform buffer too small for an asynchronous push (it does not compact)");
+    }
+    int rc = ensure_async(c);
+    if (rc) return rc;
+    // The copies land beyond every uniform the device may read until the
+    // descriptors below raise the count, so they can overlap a running step.
+    for (int i = 0; i < nsims; ++i) {
+        dvm_sim* s = sims[i];
+        if (counts[i])
+            CK(cudaMemcpyAsync(s->uniforms + s->h.ucount, u[i], 8 * counts[i],
+                               cudaMemcpyHostToDevice, c->copy_stream));
+    }
+    CK(cudaEventRecord(c->push_ev, c->copy_stream));
+    CK(cudaStreamWaitEvent(c->stream, c->push_ev, 0));
+    // Only the descriptors' uniform counts change; they go up from pinned
+    // staging, so nothing here waits for the running step (a copy from pageable
+    // memory could).  The staging is rewritten only after its previous upload.
+    CK(cudaEventSynchronize(c->ucount_ev));
+    for (int i = 0; i < nsims; ++i) {
+        dvm_sim* s = sims[i];
+        s->h.ucount += counts[i];
+        c->h_ucount[s->slot] = s->h.ucount;
+        CK(cudaMemcpyAsync(&c->d_table[s->slot].ucount, &c->h_ucount[s->slot], sizeof(uint64_t),
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaEventRecord(c->ucount_ev, c->stream));
+    return DVM_OK;
+}
+
+int dvm_batch_get_state_async(dvm_ctx* c, dvm_sim* const* sims, int nsims) {
+    if (!c || nsims < 0 || (nsims && !sims)) return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    if (c->snap_pending)
+        return fail(DVM_ERR_STATE, "a snapshot is pending: call dvm_batch_wait_state first");
+    int hi = 0;
+    uint64_t need = 0;
+    for (int i = 0; i < nsims; ++i) {
+        if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        hi = std::max(hi, sims[i]->slot + 1);
+        need += 3 * (uint64_t)sims[i]->h.cap;
+    }
+    int rc = ensure_async(c);
+    if (rc) return rc;
+    if (need > c->snap_doubles) {  // grow (stream-ordered on the compute stream)
+        if (c->snap_buf) pool_free(c, c->snap_buf);
+        c->snap_buf = nullptr;
+        c->snap_doubles = 0;
+        void* p = nullptr;
+        const cudaError_t e = pool_alloc(c, &p, 8 * need);
+        if (e != cudaSuccess) return fail(DVM_ERR_OOM, std::string("snapshot: ") + cudaGetErrorString(e));
+        c->snap_buf = static_cast<double*>(p);
+        c->snap_doubles = need;
+    }
+    c->snap_slots.assign(nsims, 0);
+    c->snap_off.assign(nsims, 0);
+    c->snap_cap.assign(nsims, 0);
+    uint64_t off = 0;
+    for (int i = 0; i < nsims; ++i) {
+        const InstDesc& h = sims[i]->h;
+        const uint64_t cap = h.cap;
+        c->snap_slots[i] = sims[i]->slot;
+        c->snap_off[i] = off;
+        c->snap_cap[i] = cap;
+        CK(cudaMemcpyAsync(c->snap_buf + off, h.x, 8 * cap, cudaMemcpyDeviceToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->snap_buf + off + cap, h.z, 8 * cap, cudaMemcpyDeviceToDevice,
+                           c->stream));
+        CK(cudaMemcpyAsync(c->snap_buf + off + 2 * cap, h.circ, 8 * cap,
+                           cudaMemcpyDeviceToDevice, c->stream));
+        off += 3 * cap;
+    }
+    if (hi)
+        CK(cudaMemcpyAsync(c->h_state_snap, c->d_state, sizeof(InstState) * (size_t)hi,
+                           cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaEventRecord(c->snap_ev, c->stream));
+    c->snap_pending = true;
+    return DVM_OK;
+}
+
+int dvm_batch_wait_state(dvm_ctx* c, int nsims, double* const* x, double* const* z,
+                         double* const* circ, const uint64_t* caps, uint64_t* counts,
+                         double* loads) {
+    if (!c || nsims < 0 || (nsims && !counts)) return fail(DVM_ERR_ARG, "bad argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    CK(cudaSetDevice(c->device));
+    if (!c->snap_pending) return fail(DVM_ERR_STATE, "no snapshot is pending");
+    if ((size_t)nsims != c->snap_slots.size())
+        return fail(DVM_ERR_ARG, "nsims differs from the pending snapshot's");
+    c->snap_pending = false;
+    CK(cudaEventSynchronize(c->snap_ev));
+    for (int i = 0; i < nsims; ++i) {  // counts and loads; sizes checked before any copy
+        const InstState& S = c->h_state_snap[c->snap_slots[i]];
+        counts[i] = S.n;
+        if (loads) {
+            loads[4 * i] = S.fx;
+            loads[4 * i + 1] = S.fz;
+            loads[4 * i + 2] = S.cd;
+            loads[4 * i + 3] = S.cl;
+        }
+        const bool any = (x && x[i]) || (z && z[i]) || (circ && circ[i]);
+        if (any && S.n && (!caps || S.n > caps[i] || S.n > c->snap_cap[i]))
+            return fail(DVM_ERR_ARG, "output capacity smaller than the blob count");
+    }
+    for (int i = 0; i < nsims; ++i) {
+        const uint64_t n = counts[i];
+        if (n == 0) continue;
+        const double* b = c->snap_buf + c->snap_off[i];
+        const uint64_t cap = c->snap_cap[i];
+        if (x && x[i]) CK(cudaMemcpyAsync(x[i], b, 8 * n, cudaMemcpyDeviceToHost, c->copy_stream));
+        if (z && z[i])
+            CK(cudaMemcpyAsync(z[i], b + cap, 8 * n, cudaMemcpyDeviceToHost, c->copy_stream));
+        if (circ && circ[i])
+            CK(cudaMemcpyAsync(circ[i], b + 2 * cap, 8 * n, cudaMemcpyDeviceToHost,
+                               c->copy_stream));
+    }
+    CK(cudaStreamSynchronize(c->copy_stream));
     return DVM_OK;
 }
 

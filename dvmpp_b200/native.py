@@ -308,6 +308,39 @@ class Context:
         cnt = (C.c_uint64 * n)(*[int(k) for k in counts])
         _check(self.lib.dvm_batch_push_uniforms(self.h, self._sim_array(sims), n, arr, cnt))
 
+    def batch_push_uniforms_async(self, sims, bufs, counts):
+        """Append uniforms on the copy stream without waiting (bufs: pinned
+        float64 arrays, unchanged until the next batch_wait_state); the next
+        enqueued step waits for the copies.  Never compacts the stream."""
+        n = len(sims)
+        P = C.POINTER(C.c_double)
+        arr = (P * n)(*[_p(b) for b in bufs])
+        cnt = (C.c_uint64 * n)(*[int(k) for k in counts])
+        _check(self.lib.dvm_batch_push_uniforms_async(self.h, self._sim_array(sims), n, arr, cnt))
+
+    def batch_get_state_async(self, sims):
+        """Snapshot the state of sims on the GPU after the enqueued work (no wait)."""
+        self._snap_n = len(sims)
+        _check(self.lib.dvm_batch_get_state_async(self.h, self._sim_array(sims), len(sims)))
+
+    def batch_wait_state(self, xs=None, zs=None, cs=None):
+        """Wait for the pending snapshot and copy it out (while later enqueued
+        steps run).  Returns (counts, loads[nsims, 4])."""
+        n = getattr(self, "_snap_n", 0)
+        P = C.POINTER(C.c_double)
+
+        def ptrs(bufs):
+            return None if bufs is None else (P * n)(*[_p(b) for b in bufs])
+
+        given = [arr for arr in (xs, zs, cs) if arr is not None]
+        caps = (C.c_uint64 * max(n, 1))(*[min(a[i].size for a in given) if given else 0
+                                          for i in range(n)])
+        counts = (C.c_uint64 * max(n, 1))()
+        loads = np.empty((n, 4))
+        _check(self.lib.dvm_batch_wait_state(self.h, n, ptrs(xs), ptrs(zs), ptrs(cs), caps, counts,
+                                             _p(loads)))
+        return [int(counts[i]) for i in range(n)], loads
+
     def batch_status(self, sims) -> list:
         out = (C.c_int32 * max(len(sims), 1))()
         _check(self.lib.dvm_batch_status(self.h, self._sim_array(sims), len(sims), out))
@@ -593,6 +626,11 @@ SIGNATURES.update({
                                       _dp]),
     "dvm_batch_push_uniforms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                           C.POINTER(C.c_uint64)]),
+    "dvm_batch_push_uniforms_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                                C.POINTER(C.c_uint64)]),
+    "dvm_batch_get_state_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "dvm_batch_wait_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp]),
     "dvm_sim_probe": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, _dp, _dp, _dp]),
     "dvm_sim_merge": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(C.c_uint64)]),
     "dvm_merge_blobs": (C.c_int, [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _u32p,

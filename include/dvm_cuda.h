@@ -318,6 +318,35 @@ int dvm_batch_get_state(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, double* c
  * values for simulation i). */
 int dvm_batch_push_uniforms(dvm_ctx* ctx, dvm_sim* const* sims, int nsims, const double* const* u,
                             const uint64_t* counts);
+/* Pipelined host loops (no counterpart in the reference, whose state lives on
+ * the host): these three calls let the copies of one step's inputs and results
+ * cross PCIe on a second stream while the GPU computes the neighbouring step.
+ * None of them waits for the GPU's compute.
+ *
+ * dvm_batch_push_uniforms_async: appends counts[i] uniforms from u[i] (pinned
+ * host memory, left unchanged until dvm_batch_wait_state or a synchronising
+ * call returns) to each simulation's injected stream; the next step enqueued
+ * after the call waits for these copies.  It never compacts the stream, so
+ * every simulation needs room in its rng_capacity for all uniforms pushed
+ * since the last synchronous push (DVM_ERR_CAPACITY otherwise, nothing copied).
+ *
+ * dvm_batch_get_state_async: snapshots x, z, circ, the blob counts and the
+ * loads of the listed simulations on the GPU after the work enqueued so far
+ * (a device-side copy), without waiting.  One snapshot per context may be
+ * pending (DVM_ERR_STATE otherwise).
+ *
+ * dvm_batch_wait_state: waits for the pending snapshot, copies the first
+ * counts[i] values of x, z, circ of the i-th listed simulation into x[i], z[i],
+ * circ[i] (pinned host memory of caps[i] values; arrays or entries may be
+ * null) on the second stream -- while later enqueued steps run -- and fills
+ * counts[i] and, if non-null, loads[4 i ..] (fx, fz, Cd, Cl).  nsims must
+ * equal the snapshot's count. */
+int dvm_batch_push_uniforms_async(dvm_ctx* ctx, dvm_sim* const* sims, int nsims,
+                                  const double* const* u, const uint64_t* counts);
+int dvm_batch_get_state_async(dvm_ctx* ctx, dvm_sim* const* sims, int nsims);
+int dvm_batch_wait_state(dvm_ctx* ctx, int nsims, double* const* x, double* const* z,
+                         double* const* circ, const uint64_t* caps, uint64_t* counts,
+                         double* loads);
 
 /* ---- pair-kernel autotuning (no counterpart in the reference) ---------------------
  * The FP32 blob-on-blob kernel's launch shape: targets per work item, persistent
