@@ -1454,6 +1454,7 @@ int dvm_batch_get_state_async(dvm_ctx* c, dvm_sim* const* sims, int nsims) {
     int rc = ensure_async(c);
     if (rc) return rc;
     if (need > c->snap_doubles) {  // grow (stream-ordered on the compute stream)
+        CK(cudaStreamSynchronize(c->copy_stream));  // no copy-out may still read the old one
         if (c->snap_buf) pool_free(c, c->snap_buf);
         c->snap_buf = nullptr;
         c->snap_doubles = 0;
