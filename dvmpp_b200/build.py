@@ -94,12 +94,22 @@ def build_oracle(verbose=False) -> None:
     reference's own sources when they are present on this machine."""
     odir = os.path.join(ROOT, "oracle")
     targets = ["oracle"]
-    ref_present = os.path.isdir(os.environ.get("DVM_REFERENCE", "/root/reference") + "/src")
+    ref = reference_dir()
+    ref_present = ref is not None
+    extra = [f"REF={ref}"] if ref_present else []
     if ref_present:
         targets.append("ref")
-    _run(["make", "-s", "-C", odir, *targets], verbose)
+    _run(["make", "-s", "-C", odir, *targets, *extra], verbose)
     if ref_present:  # the reference's own C++ tests against the drop-in classes
-        _run(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp")], verbose)
+        _run(["make", "-s", "-C", os.path.join(ROOT, "tests", "cpp"), *extra], verbose)
+
+
+def reference_dir() -> str | None:
+    """The reference source tree (gdeskos/DVMpp): $DVM_REFERENCE, else a
+    checkout named `reference` beside this repository; None when neither
+    holds a src/ directory (the oracle is then the C restatement alone)."""
+    cand = os.environ.get("DVM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+    return cand if os.path.isdir(os.path.join(cand, "src")) else None
 
 
 def main(argv=None):

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include <cuda_profiler_api.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/dvm_cuda.h"
 #include "dvm_internal.h"
@@ -163,6 +164,9 @@ struct dvm_ctx {
     std::mutex mu;
     // CUDA-event profiling of kernel families on the ctx stream (eager steps only)
     bool profiling = false;
+    // true while a step is being captured into a graph (no NVTX ranges then:
+    // they would time the capture, not the work)
+    bool capturing = false;
     struct Rec {
         int fam;
         cudaEvent_t a, b;
@@ -391,7 +395,14 @@ int key_bits_for(int nlist) {
 }
 
 // Profiling helpers: an event pair around a kernel family on the ctx stream.
+// NVTX range names of the kernel families (DVM_PROF_*), one range per phase
+// of every eagerly issued step, for an external timeline profiler.
+const char* const kNvtxNames[DVM_PROF_FAMILIES] = {
+    "dvm.biot_savart", "dvm.rhs", "dvm.sheet_solve", "dvm.sheet_velocity_convect",
+    "dvm.diffuse_release", "dvm.surface_cross", "dvm.loads", "dvm.sort_pack_combine", "dvm.step"};
+
 int prof_begin(dvm_ctx* c, int fam) {
+    if (!c->capturing) nvtxRangePushA(kNvtxNames[fam]);
     if (!c->profiling) return -1;
     cudaEvent_t a, b;
     if (c->pool.size() >= 2) {
@@ -409,6 +420,7 @@ int prof_begin(dvm_ctx* c, int fam) {
 }
 
 void prof_end(dvm_ctx* c, int idx) {
+    if (!c->capturing) nvtxRangePop();
     if (idx < 0) return;
     cudaEventRecord(c->pending[idx].b, c->stream);
 }
@@ -601,7 +613,9 @@ int run_steps(dvm_ctx* c, const std::vector<int>& slots, int nsteps, bool use_gr
         }
         if (use_graph && pl->warmed) {  // capture only after one eager step of this plan
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            c->capturing = true;
             issue_step(c, *pl);
+            c->capturing = false;
             cudaGraph_t g = nullptr;
             CK(cudaStreamEndCapture(c->stream, &g));
             cudaGraphExec_t ex = nullptr;
@@ -642,6 +656,58 @@ void host_geometry(dvm_sim* s, const double* xp, const double* zp, int npts) {
         s->enx[i] = dz / s->ds[i];
         s->enz[i] = -dx / s->ds[i];
     }
+}
+
+// A body contour the panel method can use: finite coordinates, closed (the
+// last point repeats the first, the reference's domain_file format,
+// src/VortexSheet.cpp:56-76), at least 3 panels, and no panel of zero length
+// (ds divides the normals, src/VortexSheet.cpp:93-96, and the influence
+// coefficients).  The reference does not check these; an open contour or a
+// repeated point silently gives a singular or meaningless system there.
+// Returns an empty string when the contour is valid, else the reason.
+std::string body_problem(const double* xp, const double* zp, int npts) {
+    if (npts < 4) return "a closed body needs at least 3 panels (4 points, the first repeated last)";
+    double xmn = xp[0], xmx = xp[0], zmn = zp[0], zmx = zp[0];
+    for (int i = 0; i < npts; ++i) {
+        if (!std::isfinite(xp[i]) || !std::isfinite(zp[i]))
+            return "body point " + std::to_string(i) + " is not finite";
+        xmn = std::min(xmn, xp[i]);
+        xmx = std::max(xmx, xp[i]);
+        zmn = std::min(zmn, zp[i]);
+        zmx = std::max(zmx, zp[i]);
+    }
+    const double L = std::max(xmx - xmn, zmx - zmn);
+    if (!(L > 0)) return "body points are all the same";
+    const double tol = 1e-12 * L;
+    if (std::fabs(xp[npts - 1] - xp[0]) > tol || std::fabs(zp[npts - 1] - zp[0]) > tol)
+        return "body contour is not closed: its last point must repeat the first";
+    for (int i = 0; i + 1 < npts; ++i)
+        if (std::hypot(xp[i + 1] - xp[i], zp[i + 1] - zp[i]) <= tol)
+            return "body panel " + std::to_string(i) + " has zero length (repeated point)";
+    return std::string();
+}
+
+// Serialises calls on one simulation's context (its host-side descriptor and
+// stream) and makes its device current, for the per-simulation entry points.
+struct SimLock {
+    std::lock_guard<std::mutex> lk;
+    cudaError_t dev;
+    explicit SimLock(dvm_sim* s) : lk(s->ctx->mu), dev(cudaSetDevice(s->ctx->device)) {}
+};
+#define SIM_LOCK(s)                                                         \
+    SimLock sim_lock_(s);                                                   \
+    if (sim_lock_.dev != cudaSuccess)                                       \
+        return fail(DVM_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(sim_lock_.dev))
+
+// Rejects a list that names one simulation twice (the batched pushes and
+// reads would otherwise reuse one offset or one stale cursor for both).
+int check_distinct(dvm_ctx* c, dvm_sim* const* sims, int nsims) {
+    std::vector<char> seen(kTableCap, 0);
+    for (int i = 0; i < nsims; ++i) {
+        if (!sims[i] || sims[i]->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
+        if (seen[sims[i]->slot]++) return fail(DVM_ERR_ARG, "a simulation is listed twice");
+    }
+    return DVM_OK;
 }
 
 }  // namespace
@@ -909,9 +975,16 @@ int dvm_sim_bytes(const dvm_sim_params* p, int np, uint64_t* bytes) {
 
 int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const double* bz,
                    int npts, dvm_sim** out) {
-    if (!c || !p || !bx || !bz || !out) return fail(DVM_ERR_ARG, "null argument");
+    if (!p || !bx || !bz || !out) return fail(DVM_ERR_ARG, "null argument");
     *out = nullptr;
-    if (npts < 3) return fail(DVM_ERR_ARG, "body needs at least 3 points (2 panels)");
+    // the body and the parameters are checked before the context, so a caller
+    // (or a test without a GPU) learns about a bad contour from its message
+    if (npts < 0) return fail(DVM_ERR_ARG, "negative point count");
+    const std::string why = body_problem(bx, bz, npts);
+    if (!why.empty()) return fail(DVM_ERR_ARG, why);
+    if (!std::isfinite(p->ux) || !std::isfinite(p->uz) || !std::isfinite(p->cutoff_exp) ||
+        !std::isfinite(p->dt) || !std::isfinite(p->nu) || !std::isfinite(p->rho))
+        return fail(DVM_ERR_ARG, "non-finite parameter");
     if (p->scheme != DVM_EULER && p->scheme != DVM_RK3) return fail(DVM_ERR_ARG, "bad scheme");
     if (p->surface_cross < 0 || p->surface_cross > 2) return fail(DVM_ERR_ARG, "bad surface_cross");
     if (p->precision != DVM_F64 && p->precision != DVM_F32) return fail(DVM_ERR_ARG, "bad precision");
@@ -920,6 +993,7 @@ int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const 
     if (p->capacity == 0 || p->capacity > 0xF0000000ull) return fail(DVM_ERR_ARG, "bad capacity");
     const int np = npts - 1;
     if (np > 2048) return fail(DVM_ERR_ARG, "too many panels (max 2048)");
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
     std::lock_guard<std::mutex> lk(c->mu);
     int slot = -1;
     for (int i = 1; i < kTableCap; ++i)  // slot 0 is the plugin-call scratch
@@ -1079,6 +1153,11 @@ int dvm_sim_set_blobs(dvm_sim* s, uint64_t n, const double* x, const double* z, 
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
     if (n > s->h.cap) return fail(DVM_ERR_CAPACITY, "more blobs than the simulation's capacity");
     if (n && (!x || !z || !circ || !sigma)) return fail(DVM_ERR_ARG, "null blob array");
+    for (uint64_t i = 0; i < n; ++i)
+        if (!std::isfinite(x[i]) || !std::isfinite(z[i]) || !std::isfinite(circ[i]) ||
+            !std::isfinite(sigma[i]))
+            return fail(DVM_ERR_ARG, "blob " + std::to_string(i) + " has a non-finite value");
+    SIM_LOCK(s);
     cudaStream_t st = s->ctx->stream;
     CK(cudaStreamSynchronize(st));
     if (n) {
@@ -1101,8 +1180,24 @@ int dvm_sim_set_blobs(dvm_sim* s, uint64_t n, const double* x, const double* z, 
     return DVM_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// Blob count of a simulation (device value); caller holds the sim's lock.
+int num_blobs_locked(dvm_sim* s, uint64_t* n) {
+    uint32_t v = 0;
+    CK(cudaMemcpyAsync(&v, &s->ctx->d_state[s->slot].n, 4, cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    *n = v;
+    return DVM_OK;
+}
+}  // namespace
+
+extern "C" {
+
 int dvm_sim_num_blobs(dvm_sim* s, uint64_t* n) {
     if (!s || !n) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     uint32_t v = 0;
     CK(cudaMemcpyAsync(&v, &s->ctx->d_state[s->slot].n, 4, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1119,8 +1214,9 @@ int dvm_sim_num_panels(dvm_sim* s, int* np) {
 int dvm_sim_get_blobs(dvm_sim* s, uint64_t cap, uint64_t* n_out, double* x, double* z, double* circ,
                       double* sigma, double* u, double* w, double* uvs, double* wvs, uint32_t* id) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     uint64_t n = 0;
-    int rc = dvm_sim_num_blobs(s, &n);
+    int rc = num_blobs_locked(s, &n);
     if (rc) return rc;
     if (n_out) *n_out = n;
     if (n > cap && (x || z || circ || sigma || u || w || uvs || wvs || id))
@@ -1137,6 +1233,7 @@ int dvm_sim_get_blobs(dvm_sim* s, uint64_t cap, uint64_t* n_out, double* x, doub
 
 int dvm_sim_get_gamma(dvm_sim* s, double* g) {
     if (!s || !g) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(g, s->h.gamma, 8 * s->h.np, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
     return DVM_OK;
@@ -1144,6 +1241,7 @@ int dvm_sim_get_gamma(dvm_sim* s, double* g) {
 
 int dvm_sim_set_gamma(dvm_sim* s, const double* g) {
     if (!s || !g) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(s->h.gamma, g, 8 * s->h.np, cudaMemcpyHostToDevice, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
     return DVM_OK;
@@ -1151,6 +1249,7 @@ int dvm_sim_set_gamma(dvm_sim* s, const double* g) {
 
 int dvm_sim_get_rhs(dvm_sim* s, double* b) {
     if (!s || !b) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(b, s->h.b, 8 * (s->h.np + 1), cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
     return DVM_OK;
@@ -1158,6 +1257,7 @@ int dvm_sim_get_rhs(dvm_sim* s, double* b) {
 
 int dvm_sim_get_influence(dvm_sim* s, double* A) {
     if (!s || !A) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(A, s->h.A, 8 * (size_t)(s->h.np + 1) * s->h.np, cudaMemcpyDeviceToHost,
                        s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1179,6 +1279,7 @@ int dvm_sim_get_panels(dvm_sim* s, double* xc, double* zc, double* ds, double* t
 
 int dvm_sim_get_loads(dvm_sim* s, double* fx, double* fz, double* cd, double* cl) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     InstState st;
     CK(cudaMemcpyAsync(&st, &s->ctx->d_state[s->slot], sizeof(st), cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1191,6 +1292,7 @@ int dvm_sim_get_loads(dvm_sim* s, double* fx, double* fz, double* cd, double* cl
 
 int dvm_sim_get_step(dvm_sim* s, uint32_t* step) {
     if (!s || !step) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(step, &s->ctx->d_state[s->slot].step, 4, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
     return DVM_OK;
@@ -1198,6 +1300,7 @@ int dvm_sim_get_step(dvm_sim* s, uint32_t* step) {
 
 int dvm_sim_clear_uniforms(dvm_sim* s) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     uint64_t cursor = 0;
     CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1213,6 +1316,7 @@ int dvm_sim_clear_uniforms(dvm_sim* s) {
 
 int dvm_sim_pending_uniforms(dvm_sim* s, double* out, uint64_t cap, uint64_t* n) {
     if (!s || !n) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     uint64_t cursor = 0;
     CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1228,6 +1332,7 @@ int dvm_sim_pending_uniforms(dvm_sim* s, double* out, uint64_t cap, uint64_t* n)
 
 int dvm_sim_set_step(dvm_sim* s, uint32_t step) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].step, &step, 4, cudaMemcpyHostToDevice, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
     return DVM_OK;
@@ -1235,6 +1340,7 @@ int dvm_sim_set_step(dvm_sim* s, uint32_t step) {
 
 int dvm_sim_push_uniforms(dvm_sim* s, const double* u, uint64_t n) {
     if (!s || (n && !u)) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
     if (s->h.rng != kInject) return fail(DVM_ERR_STATE, "simulation is not in inject mode");
     cudaStream_t st = s->ctx->stream;
     if (s->ctx->copy_stream) CK(cudaStreamSynchronize(s->ctx->copy_stream));
@@ -1262,6 +1368,7 @@ int dvm_sim_push_uniforms(dvm_sim* s, const double* u, uint64_t n) {
 
 int dvm_sim_rng_position(dvm_sim* s, uint64_t* consumed, uint64_t* avail) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     uint64_t cursor = 0;
     CK(cudaMemcpyAsync(&cursor, &s->ctx->d_state[s->slot].cursor, 8, cudaMemcpyDeviceToHost, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));
@@ -1348,8 +1455,10 @@ int dvm_batch_push_uniforms(dvm_ctx* c, dvm_sim* const* sims, int nsims, const d
     if (nsims == 0) return DVM_OK;
     std::lock_guard<std::mutex> lk(c->mu);
     CK(cudaSetDevice(c->device));
+    int rc = check_distinct(c, sims, nsims);
+    if (rc) return rc;
     if (c->copy_stream) CK(cudaStreamSynchronize(c->copy_stream));  // compaction moves data
-    int rc = read_states(c, sims, nsims);
+    rc = read_states(c, sims, nsims);
     if (rc) return rc;
     const uint64_t zero = 0;
     for (int i = 0; i < nsims; ++i) {
@@ -1402,6 +1511,8 @@ int dvm_batch_push_uniforms_async(dvm_ctx* c, dvm_sim* const* sims, int nsims,
     if (nsims == 0) return DVM_OK;
     std::lock_guard<std::mutex> lk(c->mu);
     CK(cudaSetDevice(c->device));
+    int rc = check_distinct(c, sims, nsims);
+    if (rc) return rc;
     for (int i = 0; i < nsims; ++i) {  // check everything before copying anything
         dvm_sim* s = sims[i];
         if (!s || s->ctx != c) return fail(DVM_ERR_ARG, "simulation of another ctx");
@@ -1411,7 +1522,7 @@ int dvm_batch_push_uniforms_async(dvm_ctx* c, dvm_sim* const* sims, int nsims,
             return fail(DVM_ERR_CAPACITY,
                         "uniform buffer too small for an asynchronous push (it does not compact)");
     }
-    int rc = ensure_async(c);
+    rc = ensure_async(c);
     if (rc) return rc;
     // The copies land beyond every uniform the device may read until the
     // descriptors below raise the count, so they can overlap a running step.
@@ -1531,6 +1642,7 @@ int dvm_batch_wait_state(dvm_ctx* c, int nsims, double* const* x, double* const*
 
 int dvm_sim_status(dvm_sim* s) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     const int st = check_device_status(s);
     if (st < 0) return st;
     switch (st) {
@@ -1546,6 +1658,7 @@ int dvm_sim_status(dvm_sim* s) {
 
 int dvm_sim_clear_status(dvm_sim* s) {
     if (!s) return fail(DVM_ERR_ARG, "sim is null");
+    SIM_LOCK(s);
     const int z = 0;
     CK(cudaMemcpyAsync(&s->ctx->d_state[s->slot].status, &z, 4, cudaMemcpyHostToDevice, s->ctx->stream));
     CK(cudaStreamSynchronize(s->ctx->stream));

@@ -891,15 +891,6 @@ constexpr size_t kNoAllocElems = 262144;  // double2 entries: 4 MiB per device
 constexpr size_t kNoAllocJobElems = 64;   // tail entries that hold the job record
 static __device__ __align__(256) double2 g_noalloc_scratch[kNoAllocElems];
 
-struct NoAllocDevice {
-    double2* scratch = nullptr;  // device address of g_noalloc_scratch
-    int sms = 0;
-    bool ready = false;
-};
-constexpr int kNoAllocMaxDevices = 64;
-NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
-std::mutex g_noalloc_mu;
-
 __global__ void k_write_job(AtJob* dst, AtJob job) { *dst = job; }
 
 }  // namespace
@@ -925,29 +916,22 @@ extern "C" int dvm_biot_savart_at_noalloc(const double* x, const double* z, cons
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0)
         return report_error(3, "dvm_biot_savart_at_noalloc: no current CUDA device");
-    NoAllocDevice& D = g_noalloc_dev[dev];
-    {
-        // One-time set-up per device, with that device current: the address of
-        // the file-scope array (host code cannot use the symbol itself).
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!D.ready) {
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess)
-                return report_error(3, (std::string("cudaGetSymbolAddress: ") +
-                                        cudaGetErrorString(e)).c_str());
-            int sms = 0;
-            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            if (e != cudaSuccess)
-                return report_error(3, (std::string("cudaDeviceGetAttribute: ") +
-                                        cudaGetErrorString(e)).c_str());
-            D.scratch = static_cast<double2*>(p);
-            D.sms = sms;
-            D.ready = true;
-        }
-    }
+    // The array's device address, looked up with the device current on every
+    // call (host code cannot use the symbol itself).  Not cached: a device
+    // reset reloads the library's device code, and the array may then move.
+    // The first call on a device also loads that code, which is why it should
+    // come before any stream capture.
+    void* scratch_p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&scratch_p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+        return report_error(3, (std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e)).c_str());
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess)
+        return report_error(3, (std::string("cudaDeviceGetAttribute: ") + cudaGetErrorString(e)).c_str());
+    double2* const scratch = static_cast<double2*>(scratch_p);
     if (ns == 0) {  // no sources: zero velocity, as the reference's empty loop gives
         if (cudaMemsetAsync(u, 0, sizeof(double) * nt, s) != cudaSuccess ||
             cudaMemsetAsync(w, 0, sizeof(double) * nt, s) != cudaSuccess)
@@ -966,15 +950,15 @@ extern "C" int dvm_biot_savart_at_noalloc(const double* x, const double* z, cons
     J.pns = nullptr;
     J.ns = (uint32_t)ns;
     J.npad = (int)npad;
-    J.part = D.scratch;  // every entry read by k_at_combine is written by k_at first
+    J.part = scratch;  // every entry read by k_at_combine is written by k_at first
     J.circ_part = nullptr;
-    AtJob* job = reinterpret_cast<AtJob*>(D.scratch + (kNoAllocElems - kNoAllocJobElems));
+    AtJob* job = reinterpret_cast<AtJob*>(scratch + (kNoAllocElems - kNoAllocJobElems));
     k_write_job<<<1, 1, 0, s>>>(job, J);
-    if (precision == kF32) k_at<true><<<D.sms * 4, 256, 0, s>>>(job, 1);
-    else k_at<false><<<D.sms * 4, 256, 0, s>>>(job, 1);
-    const unsigned cb = (unsigned)std::min<uint64_t>((nt + 255) / 256, (uint64_t)D.sms * 8);
+    if (precision == kF32) k_at<true><<<sms * 4, 256, 0, s>>>(job, 1);
+    else k_at<false><<<sms * 4, 256, 0, s>>>(job, 1);
+    const unsigned cb = (unsigned)std::min<uint64_t>((nt + 255) / 256, (uint64_t)sms * 8);
     k_at_combine<<<std::max(1u, cb), 256, 0, s>>>(job, u, w);
-    const cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     if (e != cudaSuccess)
         return report_error(3, (std::string("dvm_biot_savart_at_noalloc launch: ") +
                                 cudaGetErrorString(e)).c_str());

@@ -525,3 +525,42 @@ void delete_inside(const InstDesc* table, InstState* st, const ListEntry* list, 
 }
 
 }  // namespace dvmk
+
+// ---- the device Philox4x32-10 on caller blocks (known-answer checks) -------------
+namespace dvmk {
+namespace {
+__global__ void k_philox_blocks(const uint32_t* __restrict__ ctr, const uint32_t* __restrict__ key,
+                                uint32_t n, uint32_t* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const U4 o = philox4x32_10(U4{ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3]},
+                                   key[2 * i], key[2 * i + 1]);
+        out[4 * i] = o.a;
+        out[4 * i + 1] = o.b;
+        out[4 * i + 2] = o.c;
+        out[4 * i + 3] = o.d;
+    }
+}
+}  // namespace
+}  // namespace dvmk
+
+extern "C" int dvm_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint64_t n,
+                                 uint32_t* out) {
+    using namespace dvmk;
+    if (n == 0) return 0;
+    if (!ctr || !key || !out) return report_error(1, "null argument");
+    if (n > (1ull << 26)) return report_error(1, "at most 2^26 blocks per call");
+    uint32_t* d = nullptr;
+    const size_t words = 10 * (size_t)n;  // ctr 4n | key 2n | out 4n
+    cudaError_t e = cudaMalloc(&d, 4 * words);
+    if (e != cudaSuccess) return report_error(e == cudaErrorMemoryAllocation ? 2 : 3, cudaGetErrorString(e));
+    if (e == cudaSuccess) e = cudaMemcpy(d, ctr, 16 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + 4 * n, key, 8 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 4096);
+        k_philox_blocks<<<blocks, 256>>>(d, d + 4 * n, (uint32_t)n, d + 6 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 6 * n, 16 * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : report_error(3, cudaGetErrorString(e));
+}

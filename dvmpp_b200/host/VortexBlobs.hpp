@@ -64,8 +64,9 @@ class VortexBlobs
     void setKernelType(const std::string& type);
     [[nodiscard]] std::string kernelType() const;
     void copyOutputConfig(const VortexBlobs& other);
-    // Vortex merging is not part of the accelerated path; this build throws
-    // dvm::AlgorithmException instead of merging.
+    // Greedy vortex merging (src/VortexBlobs.cpp:110-209) on the GPU through
+    // dvm_merge_blobs: the reference's index order and FP64 arithmetic, so the
+    // merged set is bit-identical; returns the merge count.
     unsigned merge_blobs(double threshold = 1e-5);
     // Resize every array to n (values of new entries unspecified, as set_size).
     void resize(unsigned n);

@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <filesystem>
 #include <iostream>
 #include <vector>
@@ -68,16 +69,46 @@ void VortexSheet::read_input_coord(const std::string& file) {
     std::vector<double> xs, zs;
     std::string line;
     while (std::getline(f, line)) {
+        // whitespace-separated numbers (strtod: nan and inf included, so they
+        // reach the finiteness check); a token that is not a number fails
         std::istringstream s(line);
         std::vector<double> v;
-        double d;
-        while (s >> d) v.push_back(d);
+        std::string tok;
+        while (s >> tok) {
+            char* end = nullptr;
+            const double d = std::strtod(tok.c_str(), &end);
+            if (end == tok.c_str() || *end != '\0') throw dvm::FileIOException::cannotRead(file);
+            v.push_back(d);
+        }
         if (v.empty()) continue;
         if (v.size() != 2) throw dvm::FileIOException::cannotRead(file);
         xs.push_back(v[0]);
         zs.push_back(v[1]);
     }
     if (xs.size() < 3) throw dvm::FileIOException::cannotRead(file);
+    // The panel method needs a closed contour of finite points, at least 3
+    // panels, none of zero length; the reference loads any two-column file, so
+    // these checks add a clear error where it would build a singular system.
+    const size_t npts = xs.size();
+    double L = 0.0;
+    for (size_t i = 0; i < npts; ++i) {
+        if (!std::isfinite(xs[i]) || !std::isfinite(zs[i]))
+            throw dvm::FileIOException("Invalid body contour in " + file + ": point " +
+                                       std::to_string(i) + " is not finite");
+        L = std::max({L, std::fabs(xs[i] - xs[0]), std::fabs(zs[i] - zs[0])});
+    }
+    if (npts < 4)
+        throw dvm::FileIOException("Invalid body contour in " + file +
+                                   ": a closed body needs at least 3 panels (4 points, the "
+                                   "first repeated last)");
+    const double tol = 1e-12 * L;
+    if (!(L > 0) || std::fabs(xs[npts - 1] - xs[0]) > tol || std::fabs(zs[npts - 1] - zs[0]) > tol)
+        throw dvm::FileIOException("Invalid body contour in " + file +
+                                   ": not closed (the last point must repeat the first)");
+    for (size_t i = 0; i + 1 < npts; ++i)
+        if (std::hypot(xs[i + 1] - xs[i], zs[i + 1] - zs[i]) <= tol)
+            throw dvm::FileIOException("Invalid body contour in " + file + ": panel " +
+                                       std::to_string(i) + " has zero length (repeated point)");
     m_x = Vector(xs);
     m_z = Vector(zs);
     std::cout << "Successfully loaded coordinate file with " << m_x.n_elem << " points."

@@ -46,6 +46,7 @@ struct Reader {
         for (;;) {
             skip_ws();
             if (starts("<!--")) skip_past("-->");
+            else if (starts("<![CDATA[")) skip_past("]]>");  // character data: ignored
             else if (starts("<?")) skip_past("?>");
             else if (starts("<!")) skip_past(">");
             else return;
@@ -58,6 +59,23 @@ struct Reader {
             ++i;
         if (i == b) error("expected a name");
         return s.substr(b, i - b);
+    }
+    static void append_utf8(std::string& o, unsigned long cp) {
+        if (cp < 0x80) {
+            o += (char)cp;
+        } else if (cp < 0x800) {
+            o += (char)(0xC0 | (cp >> 6));
+            o += (char)(0x80 | (cp & 0x3F));
+        } else if (cp < 0x10000) {
+            o += (char)(0xE0 | (cp >> 12));
+            o += (char)(0x80 | ((cp >> 6) & 0x3F));
+            o += (char)(0x80 | (cp & 0x3F));
+        } else {
+            o += (char)(0xF0 | (cp >> 18));
+            o += (char)(0x80 | ((cp >> 12) & 0x3F));
+            o += (char)(0x80 | ((cp >> 6) & 0x3F));
+            o += (char)(0x80 | (cp & 0x3F));
+        }
     }
     static std::string unescape(const std::string& v) {
         std::string o;
@@ -73,7 +91,14 @@ struct Reader {
             else if (ent == "amp") o += '&';
             else if (ent == "quot") o += '"';
             else if (ent == "apos") o += '\'';
-            else {
+            else if (ent.size() > 1 && ent[0] == '#') {  // &#65; or &#x41;
+                const bool hex = ent[1] == 'x' || ent[1] == 'X';
+                char* end = nullptr;
+                const unsigned long cp = std::strtoul(ent.c_str() + (hex ? 2 : 1), &end, hex ? 16 : 10);
+                if (!end || *end != '\0' || cp == 0 || cp > 0x10FFFF)
+                    throw std::runtime_error("bad character reference &" + ent + ";");
+                append_utf8(o, cp);
+            } else {
                 o += v[k];
                 continue;
             }

@@ -601,6 +601,20 @@ class TuneResult(C.Structure):
                 ("ms", C.c_double * TUNE_MAX_CANDIDATES)]
 
 
+def philox4x32_10(ctr, key):
+    """The device Philox4x32-10 on blocks: ctr (n, 4) and key (n, 2) uint32
+    arrays -> (n, 4) outputs."""
+    lib = load()
+    ctr = np.ascontiguousarray(ctr, dtype=np.uint32).reshape(-1, 4)
+    key = np.ascontiguousarray(key, dtype=np.uint32).reshape(-1, 2)
+    if ctr.shape[0] != key.shape[0]:
+        raise ValueError("ctr and key must have the same number of blocks")
+    out = np.empty_like(ctr)
+    _check(lib.dvm_philox4x32_10(ctr.ctypes.data_as(_u32p), key.ctypes.data_as(_u32p), ctr.shape[0],
+                                 out.ctypes.data_as(_u32p)))
+    return out
+
+
 def tune_candidates() -> list:
     """The autotuner's search space, in the order it times it."""
     lib = load()
@@ -647,6 +661,7 @@ SIGNATURES.update({
 SIGNATURES.update({
     "dvm_ctx_reserve": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int]),
     "dvm_random_walk": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, C.c_double, C.c_double]),
+    "dvm_philox4x32_10": (C.c_int, [_u32p, _u32p, C.c_uint64, _u32p]),
     "dvm_sim_set_step": (C.c_int, [C.c_void_p, C.c_uint32]),
     "dvm_sim_clear_uniforms": (C.c_int, [C.c_void_p]),
     "dvm_sim_pending_uniforms": (C.c_int, [C.c_void_p, _dp, C.c_uint64, C.POINTER(C.c_uint64)]),

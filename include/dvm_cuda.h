@@ -188,6 +188,14 @@ int dvm_biot_savart_at_device(dvm_ctx* ctx, const double* x, const double* z, co
 int dvm_random_walk(dvm_ctx* ctx, double* x, double* z, uint64_t n, const double* R, double nu,
                     double dt);
 
+/* The device's Philox4x32-10 generator (Salmon, Moraes, Dror, Shaw, SC'11), the
+ * one the DVM_RNG_PHILOX walk draws from, applied to n caller blocks: counter
+ * ctr[4i..4i+3] and key key[2i..2i+1] give out[4i..4i+3].  No counterpart in
+ * the reference (whose walk draws from std::mt19937, src/Random.cpp:8-18); it
+ * lets a caller check the generator against published known-answer vectors.
+ * Host arrays; synchronous on the current device; n <= 2^26. */
+int dvm_philox4x32_10(const uint32_t* ctr, const uint32_t* key, uint64_t n, uint32_t* out);
+
 /* Velocity at targets without any device allocation.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot call
  * cudaMalloc: code whose device memory is owned by a host framework's
@@ -199,9 +207,11 @@ int dvm_random_walk(dvm_ctx* ctx, double* x, double* z, uint64_t n, const double
  * inside the library, which every GPU that loads the library keeps until the
  * process exits.  Limit: ceil(ns/4096) * ceil(nt/256) * 256 <= 262080 (for
  * example ns up to 1,048,576 sources with nt up to 256 targets); larger sizes
- * are rejected with DVM_ERR_ARG.  The first call on a device looks up that
- * array's device address (with the device current), so make it before any
- * stream capture.  All calls share the one array: calls that overlap on the
+ * are rejected with DVM_ERR_ARG.  Each call looks up that array's device
+ * address on the calling thread's current device (so a device reset, which
+ * may move the array, needs nothing special); the first call on a device also
+ * loads the library's device code, so make it before any stream capture.
+ * All calls share the one array: calls that overlap on the
  * GPU (different streams, or different host threads) race and corrupt each
  * other's results; serialise them on one stream.  Nothing needs clearing
  * between calls: every partial is written before it is read.  Asynchronous on

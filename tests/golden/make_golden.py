@@ -20,7 +20,7 @@ sys.path.insert(0, ROOT)
 
 from oracle.pyoracle import Ref, SimParams  # noqa: E402
 
-REFERENCE = os.environ.get("DVM_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("DVM_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
 
 
 def main():

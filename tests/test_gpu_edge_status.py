@@ -77,3 +77,52 @@ def test_injected_stream_exhausted(ctx):
     assert sim.n == 2000
     sim.clear_status()
     sim.close()
+
+
+def test_create_rejects_bad_contours_and_allocates_nothing(ctx):
+    bx, bz = W.circle(32)
+    used0 = ctx.memory()[0]
+    bad = [(bx[:-1], bz[:-1]),                                    # not closed
+           (np.insert(bx, 4, bx[4]), np.insert(bz, 4, bz[4])),    # zero-length panel
+           (np.where(np.arange(bx.size) == 3, np.nan, bx), bz),   # non-finite point
+           (np.array([0.0, 1.0, 0.0]), np.array([0.0, 0.0, 0.0]))]  # two panels
+    for xb, zb in bad:
+        with pytest.raises(N.DvmError) as e:
+            ctx.sim(_params(), xb, zb)
+        assert e.value.status == N.ERR_ARG
+    assert ctx.memory()[0] == used0
+
+
+def test_set_blobs_rejects_non_finite_and_keeps_state(ctx):
+    bx, bz = W.circle(64)
+    sim = ctx.sim(_params(), bx, bz)
+    x, z, g, s = _cloud(500, 3)
+    sim.set_blobs(x, z, g, s)
+    before = sim.blobs()
+    for arr in range(4):
+        vals = [a.copy() for a in (x, z, g, s)]
+        vals[arr][123] = np.nan if arr % 2 == 0 else np.inf
+        with pytest.raises(N.DvmError) as e:
+            sim.set_blobs(*vals)
+        assert e.value.status == N.ERR_ARG
+    after = sim.blobs()
+    assert sim.n == 500
+    for key in ("x", "z", "circ", "sigma"):
+        assert np.array_equal(before[key], after[key])
+    sim.close()
+
+
+def test_batch_pushes_reject_a_simulation_listed_twice(ctx):
+    bx, bz = W.circle(64)
+    sim = ctx.sim(_params(rng=N.RNG_INJECT, rng_capacity=1 << 12), bx, bz)
+    other = ctx.sim(_params(rng=N.RNG_INJECT, rng_capacity=1 << 12), bx, bz)
+    u = np.full(64, 0.5)
+    for push in (ctx.batch_push_uniforms, ctx.batch_push_uniforms_async):
+        with pytest.raises(N.DvmError) as e:
+            push([sim, other, sim], [u, u, u], [64, 64, 64])
+        assert e.value.status == N.ERR_ARG
+        assert sim.rng_position() == (0, 0)  # nothing was pushed
+    ctx.batch_push_uniforms([sim, other], [u, u], [64, 64])
+    assert sim.rng_position() == (0, 64) and other.rng_position() == (0, 64)
+    sim.close()
+    other.close()
