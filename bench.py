@@ -196,31 +196,39 @@ def _cores():
 
 
 class RefModel:
-    """Per-phase cost rates of the reference step, fitted on sampled
-    instances: biotsavart ~ N^2, vortexsheetbc ~ N Np (serial in the
-    reference), rest of convect ~ N Np, diffusion + crossing ~ N,
-    release + loads ~ Np."""
+    """Per-phase cost rates of the reference step, measured on sampled
+    instances and interpolated (linearly in log N, clamped at the ends) to
+    every instance of the batch: biotsavart ~ N^2, vortexsheetbc ~ N Np
+    (serial in the reference), solvevortexsheet ~ N Np, diffusion + crossing
+    ~ N, release + loads ~ Np."""
+
+    KEYS = ("a", "b", "c", "d", "e")
 
     def __init__(self):
-        self.acc = {"a": [], "b": [], "c": [], "d": [], "e": []}
+        self.samples = []  # (N, Np, rates)
 
     def add(self, N, Np, t):
-        self.acc["a"].append(t["bs"] / max(N * N, 1))
-        self.acc["b"].append(t["sbc"] / max(N * Np, 1))
-        self.acc["c"].append(max(t["convect"] - t["bs"] - t["sbc"], 0.0) / max(N * Np, 1))
-        self.acc["d"].append((t["diff"] + t["cross"]) / max(N, 1))
-        self.acc["e"].append((t["rel"] + t["loads"]) / max(Np, 1))
+        N, Np = max(N, 1), max(Np, 1)
+        self.samples.append((N, Np, {"a": t["bs"] / (N * N), "b": t["sbc"] / (N * Np),
+                                     "c": t["solve"] / (N * Np), "d": (t["diff"] + t["cross"]) / N,
+                                     "e": (t["rel"] + t["loads"]) / Np}))
+        self.samples.sort(key=lambda r: r[0])
+
+    def rates_at(self, N) -> dict:
+        xs = [math.log(r[0]) for r in self.samples]
+        lx = math.log(max(N, 1))
+        return {k: float(np.interp(lx, xs, [r[2][k] for r in self.samples])) for k in self.KEYS}
 
     def phase_times(self, instances) -> dict:
         """Seconds per batched step by phase of DVMBase::compute_step."""
-        r = {k: float(np.mean(v)) for k, v in self.acc.items()}
-        out = {"biotsavart_N2": 0.0, "vortexsheetbc_NNp": 0.0, "solve_and_update_NNp": 0.0,
+        out = {"biotsavart_N2": 0.0, "vortexsheetbc_NNp": 0.0, "solve_NNp": 0.0,
                "diffusion_and_crossing_N": 0.0, "release_and_loads_Np": 0.0}
         for inst in instances:
             N, Np = inst["nblobs"], inst["npanels"]
+            r = self.rates_at(N)
             out["biotsavart_N2"] += r["a"] * N * N
             out["vortexsheetbc_NNp"] += r["b"] * N * Np
-            out["solve_and_update_NNp"] += r["c"] * N * Np
+            out["solve_NNp"] += r["c"] * N * Np
             out["diffusion_and_crossing_N"] += r["d"] * N
             out["release_and_loads_Np"] += r["e"] * Np
         return out
@@ -228,55 +236,92 @@ class RefModel:
     def step_time(self, instances) -> float:
         return sum(self.phase_times(instances).values())
 
+    def table(self):
+        return [{"N": n, "Np": m, "s_per_pair_biotsavart": r["a"], "s_per_pair_sheetbc": r["b"],
+                 "s_per_pair_solve": r["c"], "s_per_blob_diff_cross": r["d"],
+                 "s_per_panel_release_loads": r["e"]} for n, m, r in self.samples]
 
-def ref_sample_step(ref, inst, workdir):
-    """One reference step (DVMBase::compute_step phases) on one instance, timed
-    per phase with the host clock (output writing is not part of it)."""
+
+REF_SUBSET = 4096       # targets / blobs of the sub-sampled phases on large instances
+REF_FULL_MAX = 200_000  # instances up to this size run the whole reference step
+
+
+def _ref_params():
     from oracle.pyoracle import SimParams
 
-    p = SimParams(rho=1.0, nu=1e-3, dt=0.005, ux=1.0, uz=0.0, cutoff_exp=0.675,
-                  max_numpanelvort=3, scheme="euler", surface_cross="REFLECT", seed=1, steps=10)
-    bx, bz = inst["body"]
-    s = ref.sim(p, bx, bz, workdir=workdir)
-    s.set_blobs(*inst["blobs"])
-    t = {}
+    return SimParams(rho=1.0, nu=1e-3, dt=0.005, ux=1.0, uz=0.0, cutoff_exp=0.675,
+                     max_numpanelvort=3, scheme="euler", surface_cross="REFLECT", seed=1, steps=10)
 
-    def timed(key, phase):
+
+def _timed_phases(s, keys_phases):
+    t = {}
+    for key, phase in keys_phases:
         t0 = time.perf_counter()
         s.phase(phase)
         t[key] = time.perf_counter() - t0
-
-    timed("bs", 0)
-    timed("sbc_solve", 1)
-    timed("sbc", 2)
-    timed("convect", 3)
-    timed("diff", 4)
-    timed("rel", 5)
-    timed("cross", 6)
-    timed("loads", 7)
-    # convect = biotsavart + solve + sheetbc + update; the separate bs/solve/sbc
-    # calls above measured its parts on the same state
-    t["convect"] = max(t["convect"], t["bs"] + t["sbc"])
-    del s
     return t
 
 
-def reference_sample(instances, n_samples: int, spread: bool = False):
-    """Run one reference compute_step on n_samples instances (the smallest, or
-    with spread=True, instances at evenly spaced size quantiles up to the
-    median) and extrapolate the per-phase rates to the whole batch."""
+def ref_sample_step(ref, inst, workdir):
+    """The reference's DVMBase::compute_step phases on one instance, timed with
+    the host clock (output writing is not part of it), as seconds for the
+    whole instance.  Up to REF_FULL_MAX blobs every phase runs on the whole
+    instance.  Larger instances are sampled (the N-proportional phases on a
+    subset): biotsavart as the reference's own computeInducedAt at REF_SUBSET
+    randomly chosen blobs against all N sources (the same pair loop as
+    computeSelfInduced) scaled by N / REF_SUBSET; vortexsheetbc, diffusion and
+    crossing on a REF_SUBSET-blob subset scaled likewise; solvevortexsheet as
+    its blob-free part (the normal-equations solve) plus the subset's
+    right-hand-side part scaled; release and loads as measured."""
+    p = _ref_params()
+    bx, bz = inst["body"]
+    x, z, g, sg = inst["blobs"]
+    N = x.size
+    order = [("bs", 0), ("solve", 1), ("sbc", 2), ("diff", 4), ("rel", 5), ("cross", 6),
+             ("loads", 7)]
+    if N <= REF_FULL_MAX:
+        s = ref.sim(p, bx, bz, workdir=workdir)
+        s.set_blobs(x, z, g, sg)
+        t = _timed_phases(s, order)
+        del s
+        t["how"] = "full"
+        return t
+    rng = np.random.default_rng(N)
+    pick = np.sort(rng.choice(N, REF_SUBSET, replace=False))
+    t0 = time.perf_counter()
+    ref.direct_at(x, z, g, sg, x[pick], z[pick])
+    scale = N / REF_SUBSET
+    t = {"bs": (time.perf_counter() - t0) * scale}
+    s0 = ref.sim(p, bx, bz, workdir=workdir)  # no blobs: the solve's N-free part
+    t_solve0 = _timed_phases(s0, [("solve", 1)])["solve"]
+    del s0
+    s = ref.sim(p, bx, bz, workdir=workdir)
+    s.set_blobs(x[pick], z[pick], g[pick], sg[pick])
+    ts = _timed_phases(s, order[1:])
+    del s
+    t["solve"] = t_solve0 + max(ts["solve"] - t_solve0, 0.0) * scale
+    for k in ("sbc", "diff", "cross"):
+        t[k] = ts[k] * scale
+    t["rel"], t["loads"] = ts["rel"], ts["loads"]
+    t["how"] = f"subset {REF_SUBSET}"
+    return t
+
+
+def reference_sample(instances, quantiles):
+    """One reference compute_step on the instances at the given size quantiles
+    (0 = smallest, 1 = largest) and the per-phase rates interpolated to the
+    whole batch."""
     from oracle.pyoracle import Ref, have_ref
 
     if not have_ref():
         return None
     ref = Ref()
     order = sorted(range(len(instances)), key=lambda k: instances[k]["nblobs"])
-    if spread:
-        pick = [order[(len(order) // 2) * j // max(n_samples - 1, 1)] for j in range(n_samples)]
-    else:
-        pick = order[:n_samples]
+    pick = sorted({order[round(q * (len(order) - 1))] for q in quantiles},
+                  key=lambda k: instances[k]["nblobs"])
     model = RefModel()
     total = 0.0
+    how = []
     with tempfile.TemporaryDirectory(prefix="dvmref_") as wd:
         for k in pick:
             inst = instances[k]
@@ -284,9 +329,18 @@ def reference_sample(instances, n_samples: int, spread: bool = False):
             tt = ref_sample_step(ref, inst, wd)
             total += time.perf_counter() - t0
             model.add(inst["nblobs"], inst["npanels"], tt)
+            how.append({"N": inst["nblobs"], "Np": inst["npanels"], "how": tt["how"]})
     batch = model.step_time(instances)
-    return {"batch_step_s": batch, "sampled": [instances[k]["nblobs"] for k in pick],
-            "wall_s": total, "phases_s": model.phase_times(instances)}
+    return {"batch_step_s": batch, "sampled": how, "wall_s": total,
+            "phases_s": model.phase_times(instances), "rates": model.table()}
+
+
+REF_SAMPLE_NOTE = ("DVMBase::compute_step phases of the reference, timed per phase (output "
+                   "writing off; the O(N) position update of convect not timed); instances up "
+                   f"to {REF_FULL_MAX} blobs run whole, larger ones on {REF_SUBSET}-blob "
+                   "subsets (biotsavart as computeInducedAt at that many targets against all "
+                   "sources) scaled by N / subset; per-phase rates interpolated in log N "
+                   "across the sampled sizes to all instances")
 
 
 def run_reference_arm(args, dist):
@@ -302,14 +356,13 @@ def run_reference_arm(args, dist):
         return
     os.environ.setdefault("OMP_NUM_THREADS", str(_cores()))
     for _ in range(args.warmup):
-        reference_sample(instances, 1)
+        reference_sample(instances, [0.0])
     times = []
-    sampled = []
     phases = []
+    r = None
     for k in range(args.steps):
-        r = reference_sample(instances, 1 + (k % 2))
+        r = reference_sample(instances, [0.0, 0.5, 1.0])
         times.append(r["batch_step_s"])
-        sampled.append(r["sampled"])
         phases.append(r["phases_s"])
     step_s = float(np.median(times))
     value = args.instances / step_s
@@ -323,9 +376,10 @@ def run_reference_arm(args, dist):
                                "blobs, Euler dt=0.005, REFLECT", "instances": args.instances,
                    "parallelism": "OpenMP host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": _cores(), "kind": kind,
-                         "sample": "each step: one reference DVMBase::compute_step, phase-timed, "
-                                   "on the 1-2 smallest instances; per-phase rates extrapolated "
-                                   "to all 64 instances by N^2, N*Np, N, Np",
+                         "sample": "each step: the smallest, the median and the largest "
+                                   "instance; " + REF_SAMPLE_NOTE,
+                         "sampled": r["sampled"] if r else [],
+                         "rates_last_step": r["rates"] if r else [],
                          "s_per_step_by_phase": {k: float(np.median([p[k] for p in phases]))
                                                  for k in phases[0]} if phases else {}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -357,6 +411,107 @@ def peaks():
         return {}
 
 
+ACC_REL_L2 = 1e-5     # the metric's velocity bound, per field and per simulation
+ACC_FORCE_REL = 5e-3  # Cd / Cl within 0.5 % (of the force coefficient's magnitude)
+
+
+def _rel(a, b):
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / nb if nb > 0 else float(np.linalg.norm(a - b))
+
+
+def _max_rel(a, b):
+    mb = float(np.max(np.abs(b))) if b.size else 0.0
+    return float(np.max(np.abs(a - b))) / mb if mb > 0 else 0.0
+
+
+def evaluate(sim, N):
+    """Velocity fields, panel strengths and loads of a simulation's current
+    state, without moving it: biotsavart, solvevortexsheet, vortexsheetbc
+    (no convection) and compute_loads through the phase API."""
+    for ph in (N.PHASE_BIOTSAVART, N.PHASE_SOLVE, N.PHASE_SHEETBC, N.PHASE_LOADS):
+        sim.phase(ph)
+    d = sim.blobs()
+    return d, sim.gamma(), sim.loads()
+
+
+def accuracy_vs_f64(ctx, sims, bodies, params):
+    """The timed FP32-compensated arithmetic against FP64 on the identical
+    state of every simulation of the batch: each FP32 simulation evaluates its
+    current state in place (the same kernels and source chunking as its
+    batched step); an FP64 copy of that state (same body and capacity) does
+    the same in the reference's operation order.  Per simulation: rel-L2 and
+    max-norm errors of u, w (blob-on-blob), uvs, wvs (sheet-on-blob), the total
+    induced velocity (u + uvs, w + wvs) and gamma; Cd and Cl errors relative to
+    the force coefficient's magnitude |(Cd, Cl)|."""
+    from dvmpp_b200 import native as N
+
+    fields = ("u", "w", "uvs", "wvs")
+    per = []
+    sq = {k: [0.0, 0.0] for k in fields + ("vel_total", "gamma")}
+    for sim, (bx, bz), p in zip(sims, bodies, params):
+        d32, g32, l32 = evaluate(sim, N)
+        p64 = N.Params(**{**p.__dict__, "precision": N.F64, "rng": N.RNG_PHILOX})
+        ref = ctx.sim(p64, bx, bz)
+        ref.set_blobs(d32["x"], d32["z"], d32["circ"], d32["sigma"])
+        d64, g64, l64 = evaluate(ref, N)
+        ref.close()
+        row = {"n": int(d32["x"].size), "np": int(g32.size)}
+        pairs = [(k, d32[k], d64[k]) for k in fields]
+        pairs.append(("vel_total", np.concatenate([d32["u"] + d32["uvs"], d32["w"] + d32["wvs"]]),
+                      np.concatenate([d64["u"] + d64["uvs"], d64["w"] + d64["wvs"]])))
+        pairs.append(("gamma", g32, g64))
+        for k, a, b in pairs:
+            row[k + "_rel_l2"] = _rel(a, b)
+            row[k + "_max"] = _max_rel(a, b)
+            sq[k][0] += float(np.sum((a - b) ** 2))
+            sq[k][1] += float(np.sum(b ** 2))
+        cmag = math.hypot(l64[2], l64[3])
+        row["cd_f32"], row["cd_f64"], row["cl_f32"], row["cl_f64"] = l32[2], l64[2], l32[3], l64[3]
+        row["cd_err"] = abs(l32[2] - l64[2]) / cmag if cmag > 0 else 0.0
+        row["cl_err"] = abs(l32[3] - l64[3]) / cmag if cmag > 0 else 0.0
+        per.append(row)
+    worst = {k + "_rel_l2": max(r[k + "_rel_l2"] for r in per) for k in sq}
+    worst.update({k + "_max": max(r[k + "_max"] for r in per) for k in sq})
+    worst["cd_err"] = max(r["cd_err"] for r in per)
+    worst["cl_err"] = max(r["cl_err"] for r in per)
+    pooled = {k: math.sqrt(v[0] / v[1]) if v[1] > 0 else 0.0 for k, v in sq.items()}
+    ok = (all(worst[k + "_rel_l2"] <= ACC_REL_L2 for k in sq)
+          and worst["cd_err"] <= ACC_FORCE_REL and worst["cl_err"] <= ACC_FORCE_REL)
+    return {"simulations": len(per), "blobs": int(sum(r["n"] for r in per)),
+            "how": "FP32 step arithmetic vs FP64 (reference operation order) on the identical "
+                   "state of every simulation after the timed steps; rel-L2 per simulation (worst "
+                   "shown) and pooled over all blobs; Cd / Cl error relative to |(Cd, Cl)| of FP64",
+            "bounds": {"rel_l2": ACC_REL_L2, "cd_cl": ACC_FORCE_REL},
+            "worst": worst, "pooled_rel_l2": pooled, "within_bounds": bool(ok),
+            "per_simulation": per}
+
+
+def run_f64(ctx, instances, steps_total, warmup, steps):
+    """The same batch with every pair sum in FP64 (reference operation order):
+    fresh simulations from the same initial state, Philox walk; graph-replayed
+    batched steps timed with CUDA events on the library's stream."""
+    from dvmpp_b200 import native as N
+
+    sims = []
+    for inst in instances:
+        p = sim_params(inst, steps_total, 0)
+        p.precision, p.rng = N.F64, N.RNG_PHILOX
+        s = ctx.sim(p, *inst["body"])
+        s.set_blobs(*inst["blobs"])
+        sims.append(s)
+    ctx.step_batch(sims, warmup, use_graph=True)
+    ctx.sync()
+    ctx.mark(4)
+    ctx.step_batch(sims, steps, use_graph=True)
+    ctx.mark(5)
+    ms = ctx.elapsed_ms(4, 5)
+    for s in sims:
+        s.check()
+        s.close()
+    return ms
+
+
 def run_ours(args, dist):
     from dvmpp_b200 import native as N
 
@@ -366,7 +521,7 @@ def run_ours(args, dist):
     sms, ccmaj, ccmin = ctx.device_info()
     steps_total = args.warmup + args.steps + args.prof_steps + args.plain_steps + args.e2e_steps + 2
     prepush = args.warmup + args.steps + args.prof_steps + args.plain_steps + 1
-    sims = []
+    sims, bodies, sparams = [], [], []
     for inst in instances:
         p = sim_params(inst, steps_total, prepush, args.e2e_steps + 1 if args.e2e_steps else 0)
         bx, bz = inst["body"]
@@ -374,6 +529,8 @@ def run_ours(args, dist):
         s.set_blobs(*inst["blobs"])
         s.n_hint = p.capacity
         sims.append(s)
+        bodies.append((bx, bz))
+        sparams.append(p)
     rng = np.random.default_rng(1234 + dist.rank)
     for s, u in zip(sims, uniforms_for(sims, rng, prepush)):
         s.push_uniforms(u)
@@ -439,6 +596,11 @@ def run_ours(args, dist):
     pk = peaks()
     sm_max = float(pk.get("sm_max_mhz", 1965.0))
     fp32_peak = sms * 128 * 2 * sm_max * 1e6 / 1e12
+
+    # ---- accuracy of the timed arithmetic: FP64 on the identical state
+    accuracy = None
+    if not args.no_accuracy:
+        accuracy = accuracy_vs_f64(ctx, sims, bodies, sparams)
 
     # ---- plain GPU path: one simulation at a time, same kernels, no batching
     ctx.sync()
@@ -518,17 +680,27 @@ def run_ours(args, dist):
     # ---- CPU baseline (rank 0, N = 1): the reference itself, bounded sample
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        r = reference_sample(instances, 3, spread=True)
+        r = reference_sample(instances, [0.0, 0.25, 0.5, 0.75, 1.0])
         if r:
             cpu = {"value": args.instances / r["batch_step_s"], "unit": UNIT, "cores": _cores(),
                    "kind": "reference",
-                   "sample": f"one reference compute_step (phase-timed) on each of 3 "
-                             f"instances from the smallest to the median (N={r['sampled']}), per-phase rates "
-                             f"extrapolated to all {args.instances} instances; output writing "
-                             f"off; {r['wall_s']:.1f} s of CPU work",
+                   "sample": "the instances at size quantiles 0, 0.25, 0.5, 0.75 and 1; "
+                             + REF_SAMPLE_NOTE + f"; {r['wall_s']:.1f} s of CPU work",
+                   "sampled": r["sampled"], "rates": r["rates"],
                    "s_per_step_by_phase": r["phases_s"]}
 
     nblobs = [s.n for s in sims]
+    for s in sims:
+        s.close()
+    f64 = None
+    if args.f64_steps > 0:
+        f64_ms = dist.max(run_f64(ctx, instances, 3 + args.f64_steps, 1, args.f64_steps))
+        f64 = {"value": dist.world * args.instances * args.f64_steps / (f64_ms / 1e3), "unit": UNIT,
+               "steps": args.f64_steps, "ms_per_step": f64_ms / args.f64_steps,
+               "how": "the same 64 simulations from the same initial state with every pair "
+                      "sum in FP64 in the reference's operation order (the arithmetic of the "
+                      "reference arm), Philox walk, graph-replayed batched steps after one "
+                      "warm-up step; CUDA events"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup,
@@ -572,8 +744,11 @@ def run_ours(args, dist):
         line["e2e"] = e2e
     if cpu:
         line["cpu_baseline"] = cpu
-    for s in sims:
-        s.close()
+    if accuracy:
+        line["accuracy"] = accuracy
+    if f64:
+        line["f64_value"] = f64["value"]
+        line["f64"] = f64
     ctx.close()
 
     # ---- the standalone N-body configuration (N = 2^20 wake) and the serving
@@ -591,24 +766,36 @@ def run_ours(args, dist):
     if args.serve_requests and dist.world == 1:
         from dvmpp_b200 import cases
 
-        keys = ("sim_steps_per_s", "latency_p50_s", "latency_p95_s", "latency_p99_s",
-                "queue_p50_s", "peak_active", "peak_bytes", "wall_s", "admit_s", "step_s",
-                "retire_s", "ticks")
+        keys = ("requests", "completed", "failed", "sim_steps", "sim_steps_per_s",
+                "latency_p50_s", "latency_p95_s", "latency_p99_s", "queue_p50_s", "queue_p99_s",
+                "peak_active", "peak_bytes", "wall_s", "admit_s", "step_s", "retire_s", "ticks")
+        steps = tuple(args.serve_steps)
         legs = {}
-        for mode, realtime in (("realtime", True), ("saturated", False)):
-            sv = cases.run_serving(args.serve_requests, 7, 20.0, (20, 100), (64, 512), 256,
-                                   100.0, realtime, True)
-            legs[mode] = {"batched": {k: sv["batched"][k] for k in keys},
-                          "serial": {k: sv["serial"][k] for k in keys},
-                          "ratio_batched_over_serial": sv["speedup_sim_steps"]}
+        # arrivals honoured: a feeder thread submits every request at its Poisson
+        # arrival time into the running server (live intake)
+        sv = cases.run_serving(args.serve_requests, 7, 20.0, steps, (64, 512), 256, 150.0,
+                               True, False, live=True)
+        legs["realtime_live"] = {"batched": {k: sv["batched"][k] for k in keys}}
+        # throughput: every request queued at t = 0, batched vs the plain path
+        sv = cases.run_serving(args.serve_requests, 7, 20.0, steps, (64, 512), 256, 150.0,
+                               False, not args.no_serial)
+        legs["saturated"] = {m: {k: sv[m][k] for k in keys} for m in ("batched", "serial")
+                             if m in sv}
+        if "speedup_sim_steps" in sv:
+            legs["saturated"]["ratio_batched_over_serial"] = sv["speedup_sim_steps"]
         line["serving"] = {
             "requests": args.serve_requests,
-            "arrivals": "Poisson 20 req/s (seed 7); realtime honours arrival times, saturated "
-                        "queues every request at t = 0",
-            "steps": "U{20..100} (scaled from U{100..2000})", "panels": "U{64..512}",
+            "arrivals": "Poisson 20 req/s (seed 7); realtime_live: each request submitted at its "
+                        "arrival time by a host thread while the server runs (arrival stamped "
+                        "at submission); saturated: every request queued at t = 0",
+            "steps": f"U{{{steps[0]}..{steps[1]}}} (scaled from U{{100..2000}})",
+            "panels": "U{64..512}", "budget_gb": 150.0, "max_active": 256,
             "bodies": "circle / ellipse / rounded square / Joukowski", **legs}
     if dist.rank == 0:
         print(json.dumps(line))
+    if accuracy and not accuracy["within_bounds"]:
+        sys.stderr.write("accuracy outside its bounds: " + json.dumps(accuracy["worst"]) + "\n")
+        sys.exit(3)
 
 
 def main(argv=None):
@@ -621,14 +808,22 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--prof-steps", type=int, default=2)
     ap.add_argument("--plain-steps", type=int, default=1)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--f64-steps", type=int, default=2,
+                    help="timed steps of the all-FP64 batch (0: skip)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP32-vs-FP64 check of the timed state")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the built-in pair-kernel launch shape")
     ap.add_argument("--nbody-n", type=int, default=1 << 20,
                     help="standalone N-body leg size (0: skip)")
-    ap.add_argument("--serve-requests", type=int, default=40,
+    ap.add_argument("--serve-requests", type=int, default=1000,
                     help="serving leg request count (0: skip)")
+    ap.add_argument("--serve-steps", type=int, nargs=2, default=[20, 100],
+                    help="range of the serving requests' step counts")
+    ap.add_argument("--no-serial", action="store_true",
+                    help="skip the serial plain-GPU serving run")
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per pair-kernel launch from an ncu capture")
     args = ap.parse_args(argv)

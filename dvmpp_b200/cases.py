@@ -10,6 +10,7 @@ kernel's CUDA-event time, pairs/s, FP32-pipe fraction and (with both
 precisions) the FP32-vs-FP64 error.
 
     python -m dvmpp_b200.cases precision [--steps 20] [--n-wake 524288] [--panels 1024]
+                                         [--eval-every 50] [--f64-steps 150]
 
 precision: ellipse (0.5, 0.25) at 20 degrees, 1024 panels (a 1025 x 1024
 influence matrix), a 2^19-blob wake, RK3 dt = 0.002; the FP32-compensated run
@@ -96,46 +97,126 @@ def serve_params(r) -> N.Params:
                     capacity=r["steps"] * (M + 1) * r["npanels"] * 2 + 1024)
 
 
+def _reserve_for(ctx, reqs, max_active):
+    """What a deployment configures before it opens its intake: the shared
+    workspace for max_active of the largest simulations it admits, and the
+    memory pool mapped for their slabs (so admissions never grow either)."""
+    caps = sorted((serve_params(r).capacity for r in reqs), reverse=True)[:max_active]
+    slabs = sorted((N.sim_bytes(serve_params(r), r["npanels"]) for r in reqs),
+                   reverse=True)[:max_active]
+    max_np = max(r["npanels"] for r in reqs)
+    ctx.reserve(sum(caps), min(max_active, len(reqs)), max_np)
+    ctx.pool_reserve(sum(slabs) + 8 * (3 * max_np * max_np + 64 * max_np))
+
+
 def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, max_active: int,
                 budget_gb: float, realtime: bool, serial_too: bool, graph: bool = True,
-                sync: bool = True, autotune: bool = False):
+                sync: bool = True, autotune: bool = False, live: bool = False,
+                batched: bool = True):
     """The serving workload, continuous batching and (optionally) the plain
-    serial path on the same requests; returns both summaries."""
+    serial path on the same requests; returns both summaries.
+
+    live: the requests are not pre-submitted; a feeder thread submits each at
+    its Poisson arrival time while the server runs (DVM_SERVE_LIVE), so every
+    arrival is stamped by the server at submission."""
+    import threading
+
     reqs = W.serving_requests(count, seed, rate, steps_range, panels_range)
     out = {"workload": "serving", "requests": count, "rate_per_s": rate,
            "steps_range": list(steps_range), "panels_range": list(panels_range),
-           "budget_gb": budget_gb, "realtime": realtime}
-    modes = [("batched", False)] + ([("serial", True)] if serial_too else [])
+           "budget_gb": budget_gb, "realtime": realtime, "live_intake": live}
+    modes = ([("batched", False)] if batched else []) + ([("serial", True)] if serial_too else [])
     for name, serial in modes:
         ctx = N.Context(0)
         srv = N.Server(ctx, budget_bytes=int(budget_gb * 2**30), max_active=max_active)
         srv.set_option(N.SERVE_GRAPH, 1 if graph else 0)
         srv.set_option(N.SERVE_SYNC, 1 if sync else 0)
         srv.set_option(N.SERVE_AUTOTUNE, 1 if autotune else 0)
-        for r in reqs:
-            srv.submit(serve_params(r), *r["body"], r["steps"], r["arrival"])
-        srv.run(serial=serial, realtime=realtime)
+        if live:
+            _reserve_for(ctx, reqs, 1 if serial else max_active)
+            srv.set_option(N.SERVE_LIVE, 1)
+            errors = []
+
+            def feed():
+                try:
+                    t0 = time.perf_counter()
+                    for r in reqs:
+                        wait = r["arrival"] - (time.perf_counter() - t0)
+                        if wait > 0:
+                            time.sleep(wait)
+                        srv.submit(serve_params(r), *r["body"], r["steps"])
+                except Exception as e:  # reported below
+                    errors.append(e)
+                finally:
+                    srv.close_intake()
+
+            feeder = threading.Thread(target=feed)
+            feeder.start()
+            srv.run(serial=serial, realtime=True)
+            feeder.join()
+            if errors:
+                raise errors[0]
+        else:
+            for r in reqs:
+                srv.submit(serve_params(r), *r["body"], r["steps"], r["arrival"])
+            srv.run(serial=serial, realtime=realtime)
         out[name] = srv.stats()
         srv.close()
         ctx.close()
-    if serial_too:
+    if serial_too and batched:
         out["speedup_sim_steps"] = (out["batched"]["sim_steps_per_s"]
                                     / max(out["serial"]["sim_steps_per_s"], 1e-12))
     return out
 
 
+def _evaluate(sim):
+    """Fields, panel strengths, right-hand side and loads of a simulation's
+    current state without moving it (biotsavart, solvevortexsheet,
+    vortexsheetbc, compute_loads)."""
+    for ph in (N.PHASE_BIOTSAVART, N.PHASE_SOLVE, N.PHASE_SHEETBC, N.PHASE_LOADS):
+        sim.phase(ph)
+    return sim.blobs(), sim.gamma(), sim.rhs(), sim.loads()
+
+
+def _same_state_errors(ctx, sim32, params64, body):
+    """The FP32 simulation's current state evaluated in place and by an FP64
+    copy of it (same body, capacity and parameters): rel-L2 and max-norm
+    errors of u, w, uvs, wvs, gamma and the right-hand side; Cd / Cl errors."""
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    mx = lambda a, b: float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+    d32, g32, b32, l32 = _evaluate(sim32)
+    ref = ctx.sim(params64, *body)
+    ref.set_blobs(d32["x"], d32["z"], d32["circ"], d32["sigma"])
+    dd, gd, bd, ld = _evaluate(ref)
+    ref.close()
+    out = {"n": int(dd["x"].size), "gamma_rel_l2": rel(g32, gd), "gamma_max": mx(g32, gd),
+           "rhs_rel_l2": rel(b32[:-1], bd[:-1]), "rhs_max": mx(b32[:-1], bd[:-1]),
+           "kelvin_row_abs": float(abs(b32[-1] - bd[-1]))}
+    for key in ("u", "w", "uvs", "wvs"):
+        out[key + "_rel_l2"] = rel(d32[key], dd[key])
+        out[key + "_max"] = mx(d32[key], dd[key])
+    cmag = float(np.hypot(ld[2], ld[3]))
+    out.update({"cd_f32": l32[2], "cd_f64": ld[2], "cl_f32": l32[3], "cl_f64": ld[3],
+                "cd_err_of_force": abs(l32[2] - ld[2]) / cmag if cmag > 0 else 0.0,
+                "cl_err_of_force": abs(l32[3] - ld[3]) / cmag if cmag > 0 else 0.0})
+    return out
+
+
 def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
-                  incidence_deg: float = 20.0):
+                  incidence_deg: float = 20.0, eval_every: int = 0, f64_steps=None):
     """Sheet-solve precision: an ellipse (semi-axes 0.5, 0.25) at the given
     incidence, npanels panels, a wake of n_wake blobs (the N-body distribution,
     core size ds^0.675 of this body), RK3 with dt = 0.002, nu = 1e-3, ux = 1.
     One run with FP32 compensated pair sums (FP64 QR + FP64 refinement,
-    Kelvin row in FP64) beside an all-FP64 run from the same state and the
-    same Philox stream.  Reports per-step gamma / Cd / Cl differences, the
-    blob counts, the least-squares solvers against each other on one right-
-    hand side, and the velocity fields of both precisions evaluated on one
-    identical final state."""
+    Kelvin row in FP64) for `steps` steps beside an all-FP64 run from the same
+    state and the same Philox stream for the first `f64_steps` of them (all by
+    default).  Reports per-step gamma / Cd / Cl differences while both run,
+    the blob counts, the least-squares solvers against each other on one
+    right-hand side, and -- every `eval_every` steps and at the end -- the
+    FP32 run's state evaluated in both arithmetics (fields, gamma, RHS,
+    Cd / Cl on the identical state)."""
     M = 3
+    f64_steps = steps if f64_steps is None else min(f64_steps, steps)
     ctx = N.Context(0)
     bx, bz = W.ellipse(npanels, 0.5, 0.25, incidence_deg)
     ds = np.hypot(np.diff(bx), np.diff(bz))
@@ -145,12 +226,12 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
     common = dict(rho=1.0, nu=1e-3, dt=0.002, ux=1.0, uz=0.0, max_numpanelvort=M,
                   scheme=N.RK3, surface_cross=N.REFLECT, rng=N.RNG_PHILOX, seed=11,
                   capacity=cap)
+    p64 = N.Params(precision=N.F64, **common)
     sims = {name: ctx.sim(N.Params(precision=prec, **common), bx, bz)
             for name, prec in (("f32", N.F32), ("f64", N.F64))}
     for sim in sims.values():
         sim.set_blobs(x, z, g, s)
     rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
-    mx = lambda a, b: float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
     # least-squares solvers on one right-hand side (the initial wake's)
     s64 = sims["f64"]
@@ -166,22 +247,29 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
              "residual_norm_qr": float(np.linalg.norm(A @ g_qr - b)),
              "residual_norm_lstsq": float(np.linalg.norm(A @ g_ls - b))}
 
-    rows = []
+    rows, checkpoints = [], []
     t = {"f32": 0.0, "f64": 0.0}
     for k in range(steps):
-        for name, sim in sims.items():
+        active = ("f32", "f64") if k < f64_steps else ("f32",)
+        for name in active:
+            sim = sims[name]
             ctx.sync()
             t0 = time.perf_counter()
             sim.step(1)
             ctx.sync()
             t[name] += time.perf_counter() - t0
             sim.check()
-        l32, l64 = sims["f32"].loads(), sims["f64"].loads()
-        rows.append({"step": k + 1, "n_f32": sims["f32"].n, "n_f64": sims["f64"].n,
-                     "gamma_rel_l2": rel(sims["f32"].gamma(), sims["f64"].gamma()),
-                     "cd_f32": l32[2], "cd_f64": l64[2], "cl_f32": l32[3], "cl_f64": l64[3]})
+        if k < f64_steps:
+            l32, l64 = sims["f32"].loads(), sims["f64"].loads()
+            rows.append({"step": k + 1, "n_f32": sims["f32"].n, "n_f64": sims["f64"].n,
+                         "gamma_rel_l2": rel(sims["f32"].gamma(), sims["f64"].gamma()),
+                         "cd_f32": l32[2], "cd_f64": l64[2], "cl_f32": l32[3], "cl_f64": l64[3]})
+        if eval_every and ((k + 1) % eval_every == 0 or k + 1 == steps):
+            cp = _same_state_errors(ctx, sims["f32"], p64, (bx, bz))
+            cp["step"] = k + 1
+            checkpoints.append(cp)
 
-    # both precisions evaluated on one identical state (the FP64 run's final one)
+    # both precisions evaluated on one identical state (the FP64 run's last one)
     d64 = sims["f64"].blobs()
     sims["f32"].set_blobs(d64["x"], d64["z"], d64["circ"], d64["sigma"])
     fields = {}
@@ -191,6 +279,7 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
         d = sim.blobs()
         fields[name] = (d, sim.gamma(), sim.rhs())
     (d32, g32, b32), (dd, gd, bd) = fields["f32"], fields["f64"]
+    mx = lambda a, b: float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
     same_state = {"n": int(dd["x"].size), "gamma_rel_l2": rel(g32, gd), "gamma_max": mx(g32, gd),
                   "rhs_rel_l2": rel(b32[:-1], bd[:-1]), "rhs_max": mx(b32[:-1], bd[:-1]),
                   "kelvin_row_abs": float(abs(b32[-1] - bd[-1]))}
@@ -208,16 +297,28 @@ def run_precision(steps: int, n_wake: int, npanels: int = 1024, seed: int = 2,
     cd_err = max((abs(r["cd_f32"] - r["cd_f64"]) / max(abs(r["cd_f64"]), 1e-12) for r in rows),
                  default=0.0)
     cl_err = max((abs(r["cl_f32"] - r["cl_f64"]) for r in rows), default=0.0)
+    force = [float(np.hypot(r["cd_f64"], r["cl_f64"])) for r in rows]
+    cd_f = max((abs(r["cd_f32"] - r["cd_f64"]) / f for r, f in zip(rows, force) if f > 0), default=0.0)
+    cl_f = max((abs(r["cl_f32"] - r["cl_f64"]) / f for r, f in zip(rows, force) if f > 0), default=0.0)
     return {"workload": "precision", "npanels": npanels, "incidence_deg": incidence_deg,
-            "n_wake": n_wake, "sigma": sigma, "steps": steps, "scheme": "RK3", "dt": 0.002,
-            "solve": solve, "same_state": same_state,
+            "n_wake": n_wake, "sigma": sigma, "steps": steps, "f64_steps": f64_steps,
+            "scheme": "RK3", "dt": 0.002, "solve": solve, "same_state": same_state,
+            "checkpoints": checkpoints,
             "run": {"steps_with_equal_n": sum(r["n_f32"] == r["n_f64"] for r in rows),
                     "max_gamma_rel_l2": max((r["gamma_rel_l2"] for r in rows), default=0.0),
                     "max_cd_rel": cd_err, "max_cl_abs": cl_err,
+                    "max_cd_err_of_force": cd_f, "max_cl_err_of_force": cl_f,
                     "final": rows[-1] if rows else None,
+                    "n_f32_final": sims_n_final(checkpoints, rows),
                     "s_per_step_f32": t["f32"] / max(steps, 1),
-                    "s_per_step_f64": t["f64"] / max(steps, 1)},
+                    "s_per_step_f64": t["f64"] / max(f64_steps, 1)},
             "per_step": rows}
+
+
+def sims_n_final(checkpoints, rows):
+    if checkpoints:
+        return checkpoints[-1]["n"]
+    return rows[-1]["n_f32"] if rows else None
 
 
 def run_sheet(n: int, npanels: int, reps: int, seed: int = 2):
@@ -270,6 +371,8 @@ def main(argv=None):
     sv.add_argument("--no-sync", action="store_true")
     sv.add_argument("--autotune", action="store_true",
                     help="tune the pair kernel once per new batch-shape class")
+    sv.add_argument("--live", action="store_true",
+                    help="submit each request at its arrival time while the server runs")
     sh = sub.add_parser("sheet")
     sh.add_argument("--n", type=int, default=1 << 17)
     sh.add_argument("--panels", type=int, default=1024)
@@ -279,13 +382,18 @@ def main(argv=None):
     pr.add_argument("--n-wake", type=int, default=1 << 19)
     pr.add_argument("--panels", type=int, default=1024)
     pr.add_argument("--seed", type=int, default=2)
+    pr.add_argument("--eval-every", type=int, default=0,
+                    help="evaluate the FP32 run's state in FP64 every this many steps")
+    pr.add_argument("--f64-steps", type=int, default=None,
+                    help="carry the all-FP64 run this many steps (default: all)")
     a = ap.parse_args(argv)
     if a.cmd == "precision":
-        print(json.dumps(run_precision(a.steps, a.n_wake, a.panels, a.seed)))
+        print(json.dumps(run_precision(a.steps, a.n_wake, a.panels, a.seed,
+                                       eval_every=a.eval_every, f64_steps=a.f64_steps)))
     if a.cmd == "serve":
         print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
-                                     a.max_active, a.budget_gb, a.realtime, a.serial,
-                                     not a.no_graph, not a.no_sync, a.autotune)))
+                                     a.max_active, a.budget_gb, a.realtime or a.live, a.serial,
+                                     not a.no_graph, not a.no_sync, a.autotune, a.live)))
     if a.cmd == "sheet":
         print(json.dumps(run_sheet(a.n, a.panels, a.reps)))
     if a.cmd == "nbody":

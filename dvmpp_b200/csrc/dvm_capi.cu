@@ -345,7 +345,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
                  o_work = take(64 * sizeof(unsigned)), o_flags = take(cap),
                  o_tiles = take(4 * (cap / 1024 + 1)),
                  o_tbase = take(4 * (cap / 1024 + 1)), o_kept = take(4 * 1024),
-                 o_comp = need_delete ? take(8 * 8 * cap) : take(8),
+                 o_ready = take(4 * (cap / 1024 + 1)),
                  o_jobs = take(256 * lists);
     const uint64_t bytes = off;
     if (c->in_use + bytes > c->budget)
@@ -376,7 +376,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     w.tile_counts = reinterpret_cast<uint32_t*>(b + o_tiles);
     w.tile_base = reinterpret_cast<uint32_t*>(b + o_tbase);
     w.del_kept = reinterpret_cast<uint32_t*>(b + o_kept);
-    w.compact = need_delete ? reinterpret_cast<double*>(b + o_comp) : nullptr;
+    w.del_ready = reinterpret_cast<uint32_t*>(b + o_ready);
     w.jobs = b + o_jobs;
     c->ws_cap = cap;
     c->ws_part = part;
@@ -1377,6 +1377,181 @@ int dvm_sim_rng_position(dvm_sim* s, uint64_t* consumed, uint64_t* avail) {
     return DVM_OK;
 }
 
+// ---- state save / restore ---------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// Layout of a saved simulation state (native byte order): the header, then
+// the contour (xp, zp: np+1 each), the eight blob arrays (n each), the IDs (n
+// uint32, padded to 8 bytes), gamma (np), A ((np+1) x np), P (np x (np+1)) and
+// the injected uniforms not yet consumed.
+constexpr char kStateMagic[8] = {'D', 'V', 'M', 'S', 'T', 'A', 'T', 'E'};
+constexpr uint32_t kStateVersion = 1;
+struct StateHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t header_bytes;
+    dvm_sim_params p;
+    int32_t np;
+    uint32_t n;
+    uint32_t step;
+    int32_t status;
+    uint64_t consumed_total;  // uniforms consumed since creation (inject mode)
+    uint64_t pending;         // uniforms pushed and not yet consumed
+    double fx, fz, cd, cl, totalcirc;
+    uint64_t reserved[4];
+};
+
+uint64_t state_bytes(int np, uint64_t n, uint64_t pending) {
+    const uint64_t m = (uint64_t)np;
+    return sizeof(StateHeader) + 8 * (2 * (m + 1)) + 8 * 8 * n + 8 * ((n + 1) / 2) + 8 * m +
+           16 * (m + 1) * m + 8 * pending;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dvm_sim_state_size(dvm_sim* s, uint64_t* bytes) {
+    if (!s || !bytes) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &s->ctx->d_state[s->slot], sizeof(st), cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    const uint64_t pending = s->h.ucount > st.cursor ? s->h.ucount - st.cursor : 0;
+    *bytes = state_bytes(s->h.np, st.n, pending);
+    return DVM_OK;
+}
+
+int dvm_sim_save(dvm_sim* s, void* buf, uint64_t cap, uint64_t* written) {
+    if (!s || !buf) return fail(DVM_ERR_ARG, "null argument");
+    SIM_LOCK(s);
+    cudaStream_t str = s->ctx->stream;
+    if (s->ctx->copy_stream) CK(cudaStreamSynchronize(s->ctx->copy_stream));
+    InstState st;
+    CK(cudaMemcpyAsync(&st, &s->ctx->d_state[s->slot], sizeof(st), cudaMemcpyDeviceToHost, str));
+    CK(cudaStreamSynchronize(str));
+    const int np = s->h.np;
+    const uint64_t n = st.n;
+    const uint64_t pending = s->h.ucount > st.cursor ? s->h.ucount - st.cursor : 0;
+    const uint64_t need = state_bytes(np, n, pending);
+    if (written) *written = need;
+    if (cap < need) return fail(DVM_ERR_ARG, "buffer smaller than dvm_sim_state_size");
+    StateHeader H;
+    std::memset(&H, 0, sizeof(H));
+    std::memcpy(H.magic, kStateMagic, 8);
+    H.version = kStateVersion;
+    H.header_bytes = sizeof(StateHeader);
+    H.p = s->p;
+    H.np = np;
+    H.n = st.n;
+    H.step = st.step;
+    H.status = st.status;
+    H.consumed_total = s->consumed_base + st.cursor;
+    H.pending = pending;
+    H.fx = st.fx;
+    H.fz = st.fz;
+    H.cd = st.cd;
+    H.cl = st.cl;
+    H.totalcirc = st.totalcirc;
+    char* o = static_cast<char*>(buf);
+    std::memcpy(o, &H, sizeof(H));
+    o += sizeof(H);
+    auto down = [&](const void* src, uint64_t nbytes) -> cudaError_t {
+        const cudaError_t e = nbytes ? cudaMemcpyAsync(o, src, nbytes, cudaMemcpyDeviceToHost, str)
+                                     : cudaSuccess;
+        o += nbytes;
+        return e;
+    };
+    const InstDesc& h = s->h;
+    CK(down(h.xp, 8 * (np + 1)));
+    CK(down(h.zp, 8 * (np + 1)));
+    const double* arrs[8] = {h.x, h.z, h.circ, h.sigma, h.u, h.w, h.uvs, h.wvs};
+    for (const double* a : arrs) CK(down(a, 8 * n));
+    CK(down(h.id, 4 * n));
+    if (n & 1) {
+        std::memset(o, 0, 4);
+        o += 4;
+    }
+    CK(down(h.gamma, 8 * np));
+    CK(down(h.A, 8 * (uint64_t)(np + 1) * np));
+    CK(down(h.P, 8 * (uint64_t)(np + 1) * np));
+    CK(down(s->uniforms + st.cursor, 8 * pending));
+    CK(cudaStreamSynchronize(str));
+    return DVM_OK;
+}
+
+int dvm_sim_restore(dvm_ctx* c, const void* buf, uint64_t size, dvm_sim** out) {
+    if (!c || !buf || !out) return fail(DVM_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (size < sizeof(StateHeader)) return fail(DVM_ERR_ARG, "not a saved simulation state (too short)");
+    StateHeader H;
+    std::memcpy(&H, buf, sizeof(H));
+    if (std::memcmp(H.magic, kStateMagic, 8) != 0 || H.header_bytes != sizeof(StateHeader))
+        return fail(DVM_ERR_ARG, "not a saved simulation state");
+    if (H.version != kStateVersion) return fail(DVM_ERR_ARG, "unsupported saved-state version");
+    if (H.np < 3 || H.np > 2048 || H.n > H.p.capacity)
+        return fail(DVM_ERR_ARG, "corrupt saved state (sizes)");
+    if (size != state_bytes(H.np, H.n, H.pending))
+        return fail(DVM_ERR_ARG, "saved state has the wrong size");
+    if (H.p.rng == DVM_RNG_INJECT && H.pending > std::max<uint64_t>(H.p.rng_capacity, 1))
+        return fail(DVM_ERR_ARG, "corrupt saved state (uniforms)");
+    const int np = H.np;
+    const uint64_t n = H.n;
+    const char* q = static_cast<const char*>(buf) + sizeof(H);
+    const double* xp = reinterpret_cast<const double*>(q);
+    const double* zp = xp + (np + 1);
+    dvm_sim* s = nullptr;
+    int rc = dvm_sim_create(c, &H.p, xp, zp, np + 1, &s);
+    if (rc) return rc;
+    q += 16 * (uint64_t)(np + 1);
+    {
+        SimLock lk(s);
+        cudaStream_t str = c->stream;
+        cudaError_t e = lk.dev;
+        auto up = [&](void* dst, uint64_t nbytes) {
+            if (e == cudaSuccess && nbytes)
+                e = cudaMemcpyAsync(dst, q, nbytes, cudaMemcpyHostToDevice, str);
+            q += nbytes;
+        };
+        InstDesc& h = s->h;
+        double* arrs[8] = {h.x, h.z, h.circ, h.sigma, h.u, h.w, h.uvs, h.wvs};
+        for (double* a : arrs) up(a, 8 * n);
+        up(h.id, 4 * n);
+        if (n & 1) q += 4;
+        up(h.gamma, 8 * np);
+        up(const_cast<double*>(h.A), 8 * (uint64_t)(np + 1) * np);
+        up(const_cast<double*>(h.P), 8 * (uint64_t)(np + 1) * np);
+        up(s->uniforms, 8 * H.pending);
+        InstState st;
+        std::memset(&st, 0, sizeof(st));
+        st.n = H.n;
+        st.step = H.step;
+        st.cursor = 0;
+        st.status = H.status;
+        st.fx = H.fx;
+        st.fz = H.fz;
+        st.cd = H.cd;
+        st.cl = H.cl;
+        st.totalcirc = H.totalcirc;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&c->d_state[s->slot], &st, sizeof(st), cudaMemcpyHostToDevice, str);
+        h.ucount = H.p.rng == DVM_RNG_INJECT ? H.pending : 0;
+        s->consumed_base = H.consumed_total;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->d_table + s->slot, &h, sizeof(h), cudaMemcpyHostToDevice, str);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(str);
+        if (e != cudaSuccess) rc = fail(DVM_ERR_CUDA, std::string("restore: ") + cudaGetErrorString(e));
+    }
+    if (rc) {
+        dvm_sim_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return DVM_OK;
+}
+
 // The listed simulations' InstState rows into c->h_state: one copy, one wait.
 // Call with c->mu held.
 static int read_states(dvm_ctx* c, dvm_sim* const* sims, int nsims) {
@@ -1652,6 +1827,9 @@ int dvm_sim_status(dvm_sim* s) {
             return fail(DVM_ERR_RELEASE,
                         "VortexSheet::release_nascent_vortices_rw: negative PanelNewVort");
         case kErrRngExhausted: return fail(DVM_ERR_RNG, "injected uniform stream exhausted");
+        case kErrTimeout:
+            return fail(DVM_ERR_TIMEOUT,
+                        "a bounded device wait ran out; the simulation's blobs are not consistent");
         default: return fail(st, "device status " + std::to_string(st));
     }
 }

@@ -147,7 +147,7 @@ struct Workspace {
     uint32_t* tile_counts = nullptr;  // delete: kept per 1024-tile, total_cap / 1024
     uint32_t* tile_base = nullptr;    // delete: exclusive prefix of tile_counts, per simulation
     uint32_t* del_kept = nullptr;     // delete: kept blobs per list entry
-    double* compact = nullptr;     // delete: 9 * total_cap words of staging
+    uint32_t* del_ready = nullptr;  // delete: per 1024-tile "sources read" flags
     void* jobs = nullptr;          // per-entry job records (256 B each)
     int key_bits = 40;
 };

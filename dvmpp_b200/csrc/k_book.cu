@@ -369,7 +369,10 @@ __global__ void __launch_bounds__(1024) k_del_scan(const InstState* __restrict__
     __shared__ typename Scan::TempStorage tmp;
     const ListEntry e = list[blockIdx.x];
     const InstState& S = st[e.inst];
-    if (S.status) return;
+    if (S.status) {  // a failed simulation deletes nothing (k_del_move skips it)
+        if (threadIdx.x == 0) del_kept[blockIdx.x] = S.n;
+        return;
+    }
     const uint32_t ntiles = (S.n + kDelTile - 1) / kDelTile;
     const uint32_t* tc = tile_counts + e.coff / kDelTile;
     uint32_t* tb = tile_base + e.coff / kDelTile;
@@ -385,31 +388,73 @@ __global__ void __launch_bounds__(1024) k_del_scan(const InstState* __restrict__
     if (threadIdx.x == 0) del_kept[blockIdx.x] = carry;
 }
 
-// Stable scatter of kept blobs into the staging area (8 FP64 arrays + ids).
-__global__ void __launch_bounds__(kDelTile) k_del_compact(const InstDesc* __restrict__ table,
-                                                          const InstState* __restrict__ st,
-                                                          const ListEntry* __restrict__ list,
-                                                          const uint8_t* __restrict__ flags,
-                                                          const uint32_t* __restrict__ tile_base,
-                                                          const uint32_t* __restrict__ del_kept,
-                                                          double* __restrict__ stage,
-                                                          uint64_t total_cap) {
+// Stable in-place compaction of the kept blobs (all eight FP64 arrays; IDs
+// renumbered 0..k-1, src/VortexSheet.cpp:424-437).  A kept blob moves down by
+// the number of deleted blobs before it, so tile t (kDelTile blobs) writes its
+// kept blobs to [base_t, base_t + kept_t), a range that starts inside tile
+// floor(base_t / kDelTile) <= t.  Each block takes tiles in ticket order (one
+// counter over the whole list, tiles of a simulation in increasing order),
+// loads its kept blobs into registers, publishes that its tile has been read,
+// and writes only after every lower tile its destination range overlaps has
+// published the same -- so no blob is overwritten before it has been read,
+// with no staging copy.  A tile waits only for tiles of lower tickets, which
+// blocks that are already running hold, so the waits always end; they are
+// bounded all the same, and a wait that runs out stops the simulation with
+// kErrTimeout instead of writing.  Tiles that do not move (no deletion at or
+// before them) only renumber their IDs.
+constexpr uint32_t kDelSpinLimit = 1u << 22;  // x ~100 ns: well under a second
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kDelTile) k_del_move(const InstDesc* __restrict__ table,
+                                                       InstState* __restrict__ st,
+                                                       const ListEntry* __restrict__ list,
+                                                       int nlist,
+                                                       const uint8_t* __restrict__ flags,
+                                                       const uint32_t* __restrict__ tile_base,
+                                                       const uint32_t* __restrict__ del_kept,
+                                                       uint32_t* __restrict__ ready,
+                                                       unsigned* __restrict__ ticket) {
+    __shared__ unsigned s_pre[1025];
     __shared__ uint32_t s_warp[kDelTile / 32];
-    __shared__ uint32_t s_base;
-    const ListEntry e = list[blockIdx.y];
-    const InstDesc& d = table[e.inst];
-    const InstState& S = st[e.inst];
-    if (S.status) return;
-    const uint32_t n = S.n;
-    const uint32_t ntiles = (n + kDelTile - 1) / kDelTile;
-    const uint32_t* tb = tile_base + e.coff / kDelTile;
-    if (del_kept[blockIdx.y] == n) return;  // nothing deleted: the reference returns early (:420-422)
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (threadIdx.x == 0) s_base = tb[t];        const uint32_t i = t * kDelTile + threadIdx.x;
-        const uint32_t keep = (i < n) ? flags[e.coff + i] : 0u;
-        const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ unsigned s_item;
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {  // tiles of each listed simulation that deletes something
+        // (from values no block of this launch changes, so every block agrees
+        // on which tile a ticket names)
+        unsigned acc = 0;
+        for (int k = 0; k < nlist; ++k) {
+            s_pre[k] = acc;
+            const uint32_t n = st[list[k].inst].n;
+            if (del_kept[k] != n) acc += (n + kDelTile - 1) / kDelTile;
+        }
+        s_pre[nlist] = acc;
+    }
+    __syncthreads();
+    const unsigned total = s_pre[nlist];
+    const uint32_t lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const unsigned item = s_item;
+        if (item >= total) break;
+        const int k = locate(s_pre, nlist, item);
+        const ListEntry e = list[k];
+        const InstDesc& d = table[e.inst];
+        const uint32_t n = st[e.inst].n;
+        const uint32_t t = item - s_pre[k];
+        const uint32_t tile0 = (uint32_t)(e.coff / kDelTile);
+        const uint32_t base = tile_base[tile0 + t];
+        const uint32_t i = t * kDelTile + threadIdx.x;
+        const bool keep = i < n && flags[e.coff + i] != 0;
         const uint32_t ball = __ballot_sync(0xffffffffu, keep);
-        const uint32_t before = __popc(ball & ((1u << lane) - 1u));
         if (lane == 0) s_warp[wid] = __popc(ball);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -421,43 +466,54 @@ __global__ void __launch_bounds__(kDelTile) k_del_compact(const InstDesc* __rest
             }
         }
         __syncthreads();
-        if (keep) {
-            const uint64_t o = e.coff + s_base + s_warp[wid] + before;
-            stage[0 * total_cap + o] = d.x[i];
-            stage[1 * total_cap + o] = d.z[i];
-            stage[2 * total_cap + o] = d.circ[i];
-            stage[3 * total_cap + o] = d.sigma[i];
-            stage[4 * total_cap + o] = d.u[i];
-            stage[5 * total_cap + o] = d.w[i];
-            stage[6 * total_cap + o] = d.uvs[i];
-            stage[7 * total_cap + o] = d.wvs[i];
+        const uint32_t o = base + s_warp[wid] + __popc(ball & ((1u << lane) - 1u));
+        // unmoved: nothing deleted before this tile nor inside it
+        const bool moves = __syncthreads_or(keep && o != i);
+        double v[8];
+        if (moves && keep) {
+            v[0] = d.x[i];
+            v[1] = d.z[i];
+            v[2] = d.circ[i];
+            v[3] = d.sigma[i];
+            v[4] = d.u[i];
+            v[5] = d.w[i];
+            v[6] = d.uvs[i];
+            v[7] = d.wvs[i];
+        }
+        __syncthreads();  // every source of this tile is in registers
+        if (threadIdx.x == 0) {
+            __threadfence();
+            st_release(&ready[tile0 + t], 1u);
+            int ok = 1;
+            if (moves)  // lower tiles the destination range overlaps must be read first
+                for (uint32_t u = base / kDelTile; u < t && ok; ++u) {
+                    uint32_t it = 0;
+                    while (!ld_acquire(&ready[tile0 + u])) {
+                        if (++it >= kDelSpinLimit) {
+                            ok = 0;
+                            raise_status(st[e.inst], kErrTimeout);
+                            break;
+                        }
+                        __nanosleep(100);
+                    }
+                }
+            s_ok = ok;
         }
         __syncthreads();
-    }
-}
-
-__global__ void k_del_copyback(const InstDesc* __restrict__ table, InstState* __restrict__ st,
-                               const ListEntry* __restrict__ list,
-                               const uint32_t* __restrict__ del_kept,
-                               const double* __restrict__ stage, uint64_t total_cap) {
-    const ListEntry e = list[blockIdx.y];
-    const InstDesc& d = table[e.inst];
-    const InstState& S = st[e.inst];
-    if (S.status) return;
-    const uint32_t n = S.n;
-    const uint32_t kept = del_kept[blockIdx.y];
-    if (kept == n) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < kept; i += gridDim.x * blockDim.x) {
-        const uint64_t o = e.coff + i;
-        d.x[i] = stage[0 * total_cap + o];
-        d.z[i] = stage[1 * total_cap + o];
-        d.circ[i] = stage[2 * total_cap + o];
-        d.sigma[i] = stage[3 * total_cap + o];
-        d.u[i] = stage[4 * total_cap + o];
-        d.w[i] = stage[5 * total_cap + o];
-        d.uvs[i] = stage[6 * total_cap + o];
-        d.wvs[i] = stage[7 * total_cap + o];
-        d.id[i] = i;  // IDs renumbered 0..k-1 (src/VortexSheet.cpp:429)
+        if (s_ok && keep) {
+            if (moves) {
+                d.x[o] = v[0];
+                d.z[o] = v[1];
+                d.circ[o] = v[2];
+                d.sigma[o] = v[3];
+                d.u[o] = v[4];
+                d.w[o] = v[5];
+                d.uvs[o] = v[6];
+                d.wvs[o] = v[7];
+            }
+            d.id[o] = o;  // IDs renumbered 0..k-1 (src/VortexSheet.cpp:429)
+        }
+        __syncthreads();
     }
 }
 
@@ -517,10 +573,10 @@ void delete_inside(const InstDesc* table, InstState* st, const ListEntry* list, 
     const int gx = std::max(1, sms * 4 / std::max(1, nlist));
     k_del_flags<<<dim3(gx, nlist), 256, smem, s>>>(table, st, list, ws.flags, ws.tile_counts);
     k_del_scan<<<nlist, 1024, 0, s>>>(st, list, ws.tile_counts, ws.tile_base, ws.del_kept);
-    k_del_compact<<<dim3(gx, nlist), kDelTile, 0, s>>>(table, st, list, ws.flags, ws.tile_base,
-                                                       ws.del_kept, ws.compact, ws.total_cap);
-    k_del_copyback<<<dim3(gx, nlist), 256, 0, s>>>(table, st, list, ws.del_kept, ws.compact,
-                                                   ws.total_cap);
+    cudaMemsetAsync(ws.del_ready, 0, sizeof(uint32_t) * (ws.total_cap / kDelTile + 1), s);
+    cudaMemsetAsync(ws.work + 3, 0, sizeof(unsigned), s);
+    k_del_move<<<sms * 2, kDelTile, 0, s>>>(table, st, list, nlist, ws.flags, ws.tile_base,
+                                            ws.del_kept, ws.del_ready, ws.work + 3);
     k_del_finish<<<(nlist + 127) / 128, 128, 0, s>>>(st, list, nlist, ws.del_kept);
 }
 

@@ -166,6 +166,11 @@ class Context:
         _check(self.lib.dvm_ctx_memory(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def reserve(self, total_capacity: int, max_sims: int, max_panels: int, with_delete=False):
+        """Pre-size the shared workspace for batches up to these sizes."""
+        _check(self.lib.dvm_ctx_reserve(self.h, int(total_capacity), int(max_sims),
+                                        int(max_panels), 1 if with_delete else 0))
+
     def pool_reserve(self, nbytes: int):
         """Map the stream-ordered pool for simulation slabs up to nbytes once."""
         _check(self.lib.dvm_ctx_pool_reserve(self.h, int(nbytes)))
@@ -382,6 +387,19 @@ class Context:
     def sim(self, params: "Params", xp, zp) -> "Simulation":
         return Simulation(self, params, xp, zp)
 
+    def restore(self, state: bytes, params: "Params" = None) -> "Simulation":
+        """A simulation rebuilt from Simulation.save() output (in this context)."""
+        h = C.c_void_p()
+        buf = C.create_string_buffer(bytes(state), len(state))
+        _check(self.lib.dvm_sim_restore(self.h, buf, len(state), C.byref(h)))
+        sim = Simulation.__new__(Simulation)
+        sim.ctx, sim.lib, sim.h = self, self.lib, h
+        sim.params = params
+        npn = C.c_int()
+        _check(self.lib.dvm_sim_num_panels(h, C.byref(npn)))
+        sim.np = npn.value
+        return sim
+
 
 @dataclass
 class Params:
@@ -435,6 +453,15 @@ class Simulation:
 
     def __del__(self):
         self.close()
+
+    def save(self) -> bytes:
+        """Everything a later step depends on (dvm_sim_save), as bytes."""
+        n = C.c_uint64()
+        _check(self.lib.dvm_sim_state_size(self.h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        w = C.c_uint64()
+        _check(self.lib.dvm_sim_save(self.h, buf, n.value, C.byref(w)))
+        return buf.raw[:w.value]
 
     def set_blobs(self, x, z, circ, sigma):
         x, z, circ, sigma = map(_f64, (x, z, circ, sigma))
@@ -547,7 +574,7 @@ class Simulation:
 
 
 # ---- serving ----------------------------------------------------------------
-SERVE_GRAPH, SERVE_SYNC, SERVE_AUTOTUNE = 0, 1, 2
+SERVE_GRAPH, SERVE_SYNC, SERVE_AUTOTUNE, SERVE_LIVE = 0, 1, 2, 3
 
 
 class RequestResult(C.Structure):
@@ -663,6 +690,9 @@ SIGNATURES.update({
     "dvm_random_walk": (C.c_int, [C.c_void_p, _dp, _dp, C.c_uint64, _dp, C.c_double, C.c_double]),
     "dvm_philox4x32_10": (C.c_int, [_u32p, _u32p, C.c_uint64, _u32p]),
     "dvm_sim_set_step": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "dvm_sim_state_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "dvm_sim_save": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "dvm_sim_restore": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_void_p)]),
     "dvm_sim_clear_uniforms": (C.c_int, [C.c_void_p]),
     "dvm_sim_pending_uniforms": (C.c_int, [C.c_void_p, _dp, C.c_uint64, C.POINTER(C.c_uint64)]),
     "dvm_ctx_workspace_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
@@ -673,6 +703,7 @@ SIGNATURES.update({
     "dvm_server_submit": (C.c_int, [C.c_void_p, C.POINTER(SimParams), _dp, _dp, C.c_int, C.c_uint32,
                                     C.c_double, C.POINTER(C.c_uint64)]),
     "dvm_server_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "dvm_server_close_intake": (C.c_int, [C.c_void_p]),
     "dvm_server_result": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(RequestResult)]),
     "dvm_server_final_blobs": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64),
                                          _dp, _dp, _dp]),
@@ -702,7 +733,8 @@ class Server:
     def set_option(self, option: int, value: int):
         _check(self.lib.dvm_server_set_option(self.h, option, value))
 
-    def submit(self, params: Params, xp, zp, steps: int, arrival_s: float = 0.0) -> int:
+    def submit(self, params: Params, xp, zp, steps: int, arrival_s: float = -1.0) -> int:
+        """arrival_s < 0: the request arrives when submitted."""
         xp, zp = _f64(xp), _f64(zp)
         cp = params.c()
         rid = C.c_uint64()
@@ -711,7 +743,12 @@ class Server:
         return rid.value
 
     def run(self, serial=False, realtime=False):
+        """Blocks until the run ends (ctypes releases the GIL meanwhile, so
+        other Python threads may submit)."""
         _check(self.lib.dvm_server_run(self.h, 1 if serial else 0, 1 if realtime else 0))
+
+    def close_intake(self):
+        _check(self.lib.dvm_server_close_intake(self.h))
 
     def result(self, rid: int) -> dict:
         r = RequestResult()

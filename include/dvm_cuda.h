@@ -257,6 +257,20 @@ int dvm_sim_status(dvm_sim* sim);
 int dvm_sim_clear_status(dvm_sim* sim);
 int dvm_sim_phase(dvm_sim* sim, int phase);
 int dvm_sim_step(dvm_sim* sim, int nsteps);
+/* State dump and resume (no counterpart in the reference, whose de-facto dump is
+ * the per-step text file of every blob, src/VortexBlobs.cpp:322-325, which
+ * nothing reads back).  dvm_sim_save writes everything a later step depends
+ * on into a host buffer of dvm_sim_state_size bytes: the parameters, the
+ * contour, the blob arrays (x z circ sigma u w uvs wvs, IDs), gamma, the
+ * influence matrix and its pseudo-inverse, the step counter, the status, the
+ * last loads, and the random stream's position (inject mode: the uniforms
+ * pushed but not consumed; Philox: the step counter is the position).
+ * dvm_sim_restore rebuilds the simulation in any context from such a buffer;
+ * stepping it gives the same bits as stepping the original.  Synchronous;
+ * the buffer layout is this library's (native byte order, versioned). */
+int dvm_sim_state_size(dvm_sim* sim, uint64_t* bytes);
+int dvm_sim_save(dvm_sim* sim, void* buf, uint64_t cap, uint64_t* written);
+int dvm_sim_restore(dvm_ctx* ctx, const void* buf, uint64_t size, dvm_sim** out);
 /* Vortex merging, VortexBlobs::merge_blobs (src/VortexBlobs.cpp:110-209): the
  * reference's greedy merge in index order (each surviving blob absorbs every
  * later unmerged blob with |gi gj / (gi + gj)| |xi - xj| < threshold, its state
@@ -412,7 +426,19 @@ int dvm_ctx_tuning_table(dvm_ctx* ctx, int max_entries, int* shape_classes,
  * finished ones are retired immediately and free their memory.  `serial`
  * runs the same requests one at a time (the plain GPU path) for comparison.
  * `realtime` != 0 honours arrival times on the wall clock; 0 treats every
- * request as arrived at t = 0. */
+ * request as arrived when it was submitted (t = 0 for requests submitted
+ * before the run).
+ *
+ * Requests may be submitted from other host threads while dvm_server_run
+ * works: the loop takes them in at its next tick.  Such a live request
+ * arrives at its submission time on the run's clock (or at arrival_s, if that
+ * is later); its latency counts from then.  The run returns once every
+ * submitted request has finished -- or, with DVM_SERVE_LIVE set, only after
+ * dvm_server_close_intake has been called and everything submitted before it
+ * has finished (an idle live server waits for submissions).  Submissions after
+ * the close, or after the run returned, fail with DVM_ERR_STATE.
+ * dvm_server_result may be read at any time (finished_s < 0 until the request
+ * finishes). */
 typedef struct dvm_server dvm_server;
 typedef struct {
     uint64_t id;
@@ -451,11 +477,15 @@ int dvm_server_destroy(dvm_server* srv);
 #define DVM_SERVE_GRAPH 0
 #define DVM_SERVE_SYNC 1
 #define DVM_SERVE_AUTOTUNE 2
+#define DVM_SERVE_LIVE 3 /* 1: keep running for live submissions until the intake closes */
 int dvm_server_set_option(dvm_server* srv, int option, int value);
+/* arrival_s < 0: arrives at submission (t = 0 before the run). */
 int dvm_server_submit(dvm_server* srv, const dvm_sim_params* p, const double* body_x,
                       const double* body_z, int npoints, uint32_t steps, double arrival_s,
                       uint64_t* id);
 int dvm_server_run(dvm_server* srv, int serial, int realtime);
+/* No more submissions: a live run returns once what was submitted is done. */
+int dvm_server_close_intake(dvm_server* srv);
 int dvm_server_result(dvm_server* srv, uint64_t id, dvm_request_result* out);
 int dvm_server_final_blobs(dvm_server* srv, uint64_t id, uint64_t cap, uint64_t* n, double* x,
                            double* z, double* circ);

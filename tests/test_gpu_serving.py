@@ -154,3 +154,70 @@ def test_pipelined_async_calls_match_synchronous(ctx):
     for s in a + b:
         s.check()
         s.close()
+
+
+def test_live_submissions_while_running(ctx):
+    """Requests submitted from another host thread while dvm_server_run works
+    (DVM_SERVE_LIVE) are admitted into the running batch, stamped at their
+    submission, and give the same bits as the same requests run alone."""
+    import threading
+    import time
+
+    reqs = W.serving_requests(10, seed=13, steps_range=(20, 60), panels_range=(64, 160))
+    for r in reqs[:3]:
+        r["steps"] = 150  # the early requests are still running when the live ones come
+    srv = N.Server(ctx, max_active=64, keep_state=True)
+    srv.set_option(N.SERVE_LIVE, 1)
+    early = [srv.submit(_params(r, r["steps"]), *r["body"], r["steps"]) for r in reqs[:3]]
+    errors = []
+    run = threading.Thread(target=lambda: _guard(errors, srv.run, serial=False, realtime=True))
+    run.start()
+    live = []
+    try:
+        for r in reqs[3:]:
+            time.sleep(0.05)
+            live.append(srv.submit(_params(r, r["steps"]), *r["body"], r["steps"]))
+        time.sleep(0.05)
+        srv.close_intake()
+        with pytest.raises(N.DvmError) as e:  # the intake is closed
+            srv.submit(_params(reqs[0], 5), *reqs[0]["body"], 5)
+        assert e.value.status == N.ERR_STATE
+    finally:
+        srv.close_intake()
+        run.join(timeout=300)
+    assert not run.is_alive() and not errors, errors
+    st = srv.stats()
+    assert st["completed"] == len(reqs) and st["failed"] == 0
+    results = {i: (srv.result(i), srv.final_blobs(i)) for i in early + live}
+    srv.close()
+    # live requests were submitted after the run started: stamped then, and
+    # some of them ran beside the early ones
+    starts = [results[i][0]["arrival_s"] for i in live]
+    assert all(a > 0 for a in starts) and starts == sorted(starts)
+    assert any(results[i][0]["admitted_s"] < results[early[0]][0]["finished_s"] for i in live)
+    alone, _ = _run(ctx, reqs, serial=True)
+    for k, i in enumerate(early + live):
+        (ra, (xa, za, ca)), (rb, (xb, zb, cb)) = results[i], alone[k]
+        assert ra["status"] == 0 and ra["steps_done"] == reqs[k]["steps"]
+        assert ra["blobs"] == rb["blobs"]
+        assert np.array_equal(xa, xb) and np.array_equal(za, zb) and np.array_equal(ca, cb)
+        assert ra["cd"] == rb["cd"] and ra["cl"] == rb["cl"]
+
+
+def _guard(errors, fn, **kw):
+    try:
+        fn(**kw)
+    except Exception as e:  # surfaced by the test thread
+        errors.append(e)
+
+
+def test_submit_after_run_is_refused(ctx):
+    reqs = W.serving_requests(2, seed=14, steps_range=(3, 5), panels_range=(64, 80))
+    srv = N.Server(ctx, max_active=4)
+    for r in reqs:
+        srv.submit(_params(r, r["steps"]), *r["body"], r["steps"])
+    srv.run()
+    with pytest.raises(N.DvmError) as e:
+        srv.submit(_params(reqs[0], 3), *reqs[0]["body"], 3)
+    assert e.value.status == N.ERR_STATE
+    srv.close()
