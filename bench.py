@@ -767,6 +767,7 @@ def run_ours(args, dist):
         from dvmpp_b200 import cases
 
         keys = ("requests", "completed", "failed", "sim_steps", "sim_steps_per_s",
+                "blobs_per_panel_step",
                 "latency_p50_s", "latency_p95_s", "latency_p99_s", "queue_p50_s", "queue_p99_s",
                 "peak_active", "peak_bytes", "wall_s", "admit_s", "step_s", "retire_s", "ticks")
         steps = tuple(args.serve_steps)

@@ -161,6 +161,15 @@ def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, m
                 srv.submit(serve_params(r), *r["body"], r["steps"], r["arrival"])
             srv.run(serial=serial, realtime=realtime)
         out[name] = srv.stats()
+        # blob growth: blobs at the end per (panel x step) over the completed
+        # requests (each starts empty), for extrapolating to other step ranges
+        nb = npsteps = 0
+        for rid in range(out[name]["requests"]):
+            res = srv.result(rid)
+            if res["status"] == 0 and res["steps_done"] > 0:
+                nb += res["blobs"]
+                npsteps += reqs[rid]["npanels"] * res["steps_done"]
+        out[name]["blobs_per_panel_step"] = nb / npsteps if npsteps else None
         srv.close()
         ctx.close()
     if serial_too and batched:

