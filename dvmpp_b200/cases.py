@@ -21,7 +21,12 @@ influence matrix), a 2^19-blob wake, RK3 dt = 0.002; the FP32-compensated run
 sheet: the FP32 sheet-on-blob velocity alone (ellipse at 20 degrees, wake of
 n blobs); prints its CUDA-event time, pairs/s and FP32 fraction (67 flop/pair).
 
-    python -m dvmpp_b200.cases serve [--requests 100] [--serial] [--realtime]
+    python -m dvmpp_b200.cases rhs [--n 131072] [--panels 1024] [--reps 3]
+
+rhs: the blob-on-collocation right-hand side alone (same body and wake);
+prints its CUDA-event time per launch, pairs/s and FP32 fraction (12 flop/pair).
+
+    python -m dvmpp_b200.cases serve [--requests 100] [--serial] [--realtime] [--live]
 
 serve: the continuous-batching server on Poisson arrivals (seed 7, 20 req/s).
 """
@@ -112,21 +117,25 @@ def _reserve_for(ctx, reqs, max_active):
 def run_serving(count: int, seed: int, rate: float, steps_range, panels_range, max_active: int,
                 budget_gb: float, realtime: bool, serial_too: bool, graph: bool = True,
                 sync: bool = True, autotune: bool = False, live: bool = False,
-                batched: bool = True):
+                batched: bool = True, serial_every: int = 1):
     """The serving workload, continuous batching and (optionally) the plain
     serial path on the same requests; returns both summaries.
 
     live: the requests are not pre-submitted; a feeder thread submits each at
     its Poisson arrival time while the server runs (DVM_SERVE_LIVE), so every
-    arrival is stamped by the server at submission."""
+    arrival is stamped by the server at submission.
+    serial_every: the serial path runs every k-th request only (its sim-steps/s
+    is then a rate on a sample of the same distribution)."""
     import threading
 
-    reqs = W.serving_requests(count, seed, rate, steps_range, panels_range)
+    all_reqs = W.serving_requests(count, seed, rate, steps_range, panels_range)
     out = {"workload": "serving", "requests": count, "rate_per_s": rate,
            "steps_range": list(steps_range), "panels_range": list(panels_range),
-           "budget_gb": budget_gb, "realtime": realtime, "live_intake": live}
+           "budget_gb": budget_gb, "realtime": realtime, "live_intake": live,
+           "serial_every": serial_every}
     modes = ([("batched", False)] if batched else []) + ([("serial", True)] if serial_too else [])
     for name, serial in modes:
+        reqs = all_reqs[::serial_every] if serial else all_reqs
         ctx = N.Context(0)
         srv = N.Server(ctx, budget_bytes=int(budget_gb * 2**30), max_active=max_active)
         srv.set_option(N.SERVE_GRAPH, 1 if graph else 0)
@@ -358,6 +367,38 @@ def run_sheet(n: int, npanels: int, reps: int, seed: int = 2):
             "fp32_peak_frac": tf / _fp32_peak_tflops(sms)}
 
 
+def run_rhs(n: int, npanels: int, reps: int, seed: int = 2):
+    """Blob-on-collocation right-hand side alone (the at-target kernel of
+    solvevortexsheet, src/VortexSheet.cpp:181-203): an ellipse (0.5, 0.25) at
+    20 degrees with npanels panels and an n-blob wake, FP32 instance; the
+    profiled RHS family's CUDA-event time per launch, pairs/s and the FP32
+    fraction at 12 flop per pair."""
+    ctx = N.Context(0)
+    sms, _, _ = ctx.device_info()
+    bx, bz = W.ellipse(npanels, incidence_deg=20.0)
+    x, z, g, s = W.wake(n, seed, W.core_size(bx, bz))
+    sim = ctx.sim(N.Params(capacity=n + 8 * npanels, precision=N.F32, rng=N.RNG_PHILOX, ux=1.0),
+                  bx, bz)
+    sim.set_blobs(x, z, g, s)
+    sim.step(1)  # warm-up: one whole step (the batched RHS launch included)
+    sim.set_blobs(x, z, g, s)
+    ctx.set_profiling(True)
+    ctx.profile_reset()
+    for _ in range(reps):
+        sim.step(1)
+        sim.set_blobs(x, z, g, s)
+    prof = ctx.profile()
+    ctx.set_profiling(False)
+    ms = prof["rhs"][0] / max(prof["rhs"][1], 1)
+    pairs = n * npanels
+    tf = 12.0 * pairs / (ms / 1e3) / 1e12
+    sim.close()
+    ctx.close()
+    return {"workload": "rhs", "n": n, "panels": npanels, "pairs": pairs, "kernel_ms": ms,
+            "gpairs_per_s": pairs / (ms / 1e3) / 1e9, "tflops_12_per_pair": tf,
+            "fp32_peak_frac": tf / _fp32_peak_tflops(sms)}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -382,10 +423,16 @@ def main(argv=None):
                     help="tune the pair kernel once per new batch-shape class")
     sv.add_argument("--live", action="store_true",
                     help="submit each request at its arrival time while the server runs")
+    sv.add_argument("--serial-every", type=int, default=1,
+                    help="the serial path runs every k-th request only")
     sh = sub.add_parser("sheet")
     sh.add_argument("--n", type=int, default=1 << 17)
     sh.add_argument("--panels", type=int, default=1024)
     sh.add_argument("--reps", type=int, default=3)
+    rh = sub.add_parser("rhs")
+    rh.add_argument("--n", type=int, default=1 << 17)
+    rh.add_argument("--panels", type=int, default=1024)
+    rh.add_argument("--reps", type=int, default=3)
     pr = sub.add_parser("precision")
     pr.add_argument("--steps", type=int, default=20)
     pr.add_argument("--n-wake", type=int, default=1 << 19)
@@ -402,9 +449,12 @@ def main(argv=None):
     if a.cmd == "serve":
         print(json.dumps(run_serving(a.requests, a.seed, a.rate, tuple(a.steps), tuple(a.panels),
                                      a.max_active, a.budget_gb, a.realtime or a.live, a.serial,
-                                     not a.no_graph, not a.no_sync, a.autotune, a.live)))
+                                     not a.no_graph, not a.no_sync, a.autotune, a.live,
+                                     serial_every=a.serial_every)))
     if a.cmd == "sheet":
         print(json.dumps(run_sheet(a.n, a.panels, a.reps)))
+    if a.cmd == "rhs":
+        print(json.dumps(run_rhs(a.n, a.panels, a.reps)))
     if a.cmd == "nbody":
         precs = {"f32": [N.F32], "f64": [N.F64], "both": [N.F32, N.F64]}[a.prec]
         print(json.dumps(run_nbody(a.n, precs, a.reps, a.seed)))

@@ -610,8 +610,28 @@ struct AtJob {
     double* circ_part;    // [chunk], or null
 };
 
+// Kahan sum of packed pairs with the compensation kept negated (e = -c):
+// y = x + e, t = s + y, e = y - (t - s), s = t -- each half the scalar
+// algorithm; x = a b enters through one fused multiply-add.
+__device__ __forceinline__ void kahan2_fma(uint64_t& s, uint64_t& e, uint64_t a, uint64_t b) {
+    const uint64_t y = f2fma(a, b, e);
+    const uint64_t t = f2add(s, y);
+    e = f2sub(y, f2sub(t, s));
+    s = t;
+}
+
+// Velocity at targets from a chunk of kAtChunk sources per work item.  FP32
+// path: 512 targets per item, two per thread; jobs without the close-pair skip
+// (the blob-on-collocation right-hand side) run packed FP32x2 with a per-pair
+// compensated sum (the right-hand side is the small residual normal velocity,
+// so its rounding must stay relative to the few large near-blob terms, not
+// compound) and the core kernel, when any lane of the warp has a pair inside
+// a core, for both halves with a select; the skip jobs (at-target plugin
+// calls, probes) run the scalar loop.  FP64 path: 256 targets per item, the
+// reference's operation order.
 template <bool F32>
 __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int njobs) {
+    constexpr uint32_t kTile = F32 ? 512 : 256;
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ double s_x[256], s_z[256], s_c[256], s_thr[256], s_rs[256];
     __shared__ float s_cf[256], s_thrf[256], s_rsf[256];  // FP32 copies (F32 path)
@@ -621,7 +641,7 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
         for (int k = 0; k < njobs; ++k) {
             s_pre[k] = acc;
             const uint32_t ns = jobs[k].pns ? *jobs[k].pns : jobs[k].ns;
-            acc += ((jobs[k].nt + 255) / 256) * ((ns + kAtChunk - 1) / kAtChunk);
+            acc += ((jobs[k].nt + kTile - 1) / kTile) * ((ns + kAtChunk - 1) / kAtChunk);
         }
         s_pre[njobs] = acc;
     }
@@ -634,11 +654,15 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
         const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
         const unsigned local = item - s_pre[k];
         const uint32_t ttile = local / nchunk, c = local % nchunk;
-        const uint32_t t = ttile * 256 + threadIdx.x;
-        const double tx = t < J.nt ? J.tx[t] : 0.0, tz = t < J.nt ? J.tz[t] : 0.0;
+        const uint32_t t0 = ttile * kTile + threadIdx.x, t1 = t0 + 256;  // t1: F32 only
+        const double tx0 = t0 < J.nt ? J.tx[t0] : 0.0, tz0 = t0 < J.nt ? J.tz[t0] : 0.0;
+        const double tx1 = (F32 && t1 < J.nt) ? J.tx[t1] : 0.0;
+        const double tz1 = (F32 && t1 < J.nt) ? J.tz[t1] : 0.0;
         const uint32_t j0 = c * kAtChunk, j1 = min(ns, j0 + kAtChunk);
-        double uu = 0.0, ww = 0.0, csum = 0.0;
-        float su = 0.f, cu = 0.f, sw = 0.f, cw = 0.f;
+        double uu0 = 0.0, ww0 = 0.0, uu1 = 0.0, ww1 = 0.0, csum = 0.0;
+        const uint64_t zero2 = f2pack(0.0f, 0.0f);
+        uint64_t snu = zero2, enu = zero2, sw = zero2, ew = zero2;  // -u and w, packed Kahan
+        float su[2] = {0.f, 0.f}, cu[2] = {0.f, 0.f}, sws[2] = {0.f, 0.f}, cws[2] = {0.f, 0.f};
         for (uint32_t s0 = j0; s0 < j1; s0 += 256) {
             __syncthreads();
             const uint32_t j = s0 + threadIdx.x;
@@ -659,40 +683,71 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
             }
             __syncthreads();
             const int cnt = (int)min(256u, j1 - s0);
-            if (F32) {
-                // compensated per pair: the right-hand side is the small
-                // residual normal velocity, so the sum's rounding must stay
-                // relative to the few large near-blob terms, not compound
+            if (F32 && !J.skip_close) {
                 for (int jj = 0; jj < cnt; ++jj) {
-                    const float dx = (float)(tx - s_x[jj]);
-                    const float dz = (float)(tz - s_z[jj]);
-                    const float r2 = fmaf(dx, dx, dz * dz);
-                    if (J.skip_close && !(r2 > 1e-15f)) continue;
-                    float K = rcp_approx(r2);
-                    if (r2 < s_thrf[jj]) K = core_kernel_expm1(r2, s_rsf[jj], K);
-                    const float g = K * s_cf[jj];
-                    kahan(su, cu, -g * dz);
-                    kahan(sw, cw, g * dx);
+                    const double sx = s_x[jj], sz = s_z[jj];
+                    const uint64_t DX = f2pack((float)(tx0 - sx), (float)(tx1 - sx));
+                    const uint64_t DZ = f2pack((float)(tz0 - sz), (float)(tz1 - sz));
+                    const uint64_t R2 = f2fma(DX, DX, f2mul(DZ, DZ));
+                    const float ra = f2lo(R2), rb = f2hi(R2), thr = s_thrf[jj];
+                    float ka = rcp_approx(ra), kb = rcp_approx(rb);
+                    const bool ca = ra < thr, cb = rb < thr;
+                    if (__any_sync(0xffffffffu, ca || cb)) {
+                        const float rs = s_rsf[jj];
+                        const float qa = core_kernel_expm1(ra, rs, ka);
+                        const float qb = core_kernel_expm1(rb, rs, kb);
+                        ka = ca ? qa : ka;
+                        kb = cb ? qb : kb;
+                    }
+                    const float cf = s_cf[jj];
+                    const uint64_t G = f2mul(f2pack(ka, kb), f2pack(cf, cf));
+                    kahan2_fma(snu, enu, G, DZ);
+                    kahan2_fma(sw, ew, G, DX);
+                }
+            } else if (F32) {
+                for (int h = 0; h < 2; ++h) {
+                    const double tx = h ? tx1 : tx0, tz = h ? tz1 : tz0;
+                    for (int jj = 0; jj < cnt; ++jj) {
+                        const float dx = (float)(tx - s_x[jj]);
+                        const float dz = (float)(tz - s_z[jj]);
+                        const float r2 = fmaf(dx, dx, dz * dz);
+                        if (!(r2 > 1e-15f)) continue;  // skip_close (computeInducedAt :89)
+                        float K = rcp_approx(r2);
+                        if (r2 < s_thrf[jj]) K = core_kernel_expm1(r2, s_rsf[jj], K);
+                        const float g = K * s_cf[jj];
+                        kahan(su[h], cu[h], -g * dz);
+                        kahan(sws[h], cws[h], g * dx);
+                    }
                 }
             } else {
                 for (int jj = 0; jj < cnt; ++jj) {
-                    const double dx = dsub(tx, s_x[jj]);
-                    const double dz = dsub(tz, s_z[jj]);
+                    const double dx = dsub(tx0, s_x[jj]);
+                    const double dz = dsub(tz0, s_z[jj]);
                     const double r2 = dadd(dmul(dx, dx), dmul(dz, dz));
                     if (J.skip_close && !(r2 > 1e-15)) continue;
                     double K;
                     if (r2 < s_thr[jj]) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
                     else K = __drcp_rn(r2);  // correctly rounded: the same value as 1.0 / r2
-                    uu = dsub(uu, dmul(dmul(K, dz), s_c[jj]));
-                    ww = dadd(ww, dmul(dmul(K, dx), s_c[jj]));
+                    uu0 = dsub(uu0, dmul(dmul(K, dz), s_c[jj]));
+                    ww0 = dadd(ww0, dmul(dmul(K, dx), s_c[jj]));
                 }
             }
         }
         if (F32) {
-            uu = (double)su - (double)cu;
-            ww = (double)sw - (double)cw;
+            if (!J.skip_close) {
+                uu0 = -((double)f2lo(snu) + (double)f2lo(enu));
+                uu1 = -((double)f2hi(snu) + (double)f2hi(enu));
+                ww0 = (double)f2lo(sw) + (double)f2lo(ew);
+                ww1 = (double)f2hi(sw) + (double)f2hi(ew);
+            } else {
+                uu0 = (double)su[0] - (double)cu[0];
+                ww0 = (double)sws[0] - (double)cws[0];
+                uu1 = (double)su[1] - (double)cu[1];
+                ww1 = (double)sws[1] - (double)cws[1];
+            }
+            if (t1 < J.nt) J.part[(uint64_t)c * J.npad + t1] = make_double2(uu1, ww1);
         }
-        if (t < J.nt) J.part[(uint64_t)c * J.npad + t] = make_double2(uu, ww);
+        if (t0 < J.nt) J.part[(uint64_t)c * J.npad + t0] = make_double2(uu0, ww0);
         if (ttile == 0 && J.circ_part) {
             for (int o = 16; o > 0; o >>= 1) csum += __shfl_xor_sync(0xffffffffu, csum, o);
             if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = csum;
