@@ -275,7 +275,8 @@ int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl, bool f32_pairs = false) {
         e.inst = s->slot;
         e.cap = s->h.cap;
         e.chunks = nbody_chunks(e.cap);
-        e.rhs_chunks = (int)std::max<uint64_t>(1, (e.cap + kAtChunk - 1) / kAtChunk);
+        e.rhs_chunk = rhs_chunk_for(e.cap, s->h.np);
+        e.rhs_chunks = (int)std::max<uint64_t>(1, (e.cap + e.rhs_chunk - 1) / e.rhs_chunk);
         e.npad = (int)align_up((size_t)s->h.np, 256);
         e.coff = coff;
         e.poff = poff;
@@ -853,9 +854,10 @@ int dvm_ctx_reserve(dvm_ctx* c, uint64_t total_capacity, int max_sims, int max_p
     CK(cudaSetDevice(c->device));
     const uint64_t S = (uint64_t)max_sims;
     const uint64_t T = align_up(total_capacity, kCapAlign) + S * kCapAlign;
-    // bounds of the per-list sums: chunks*cap <= 16 cap + 2^21, rhs chunks <= cap/4096 + 1
+    // bounds of the per-list sums: chunks*cap <= 16 cap + 2^21; rhs chunks per
+    // simulation <= 601 or cap / kAtChunk + 1 (rhs_chunk_for)
     const uint64_t part = 16 * T + S * (2u << 20);
-    const uint64_t rchunks = T / kAtChunk + S;
+    const uint64_t rchunks = T / kAtChunk + S * 602;
     return ensure_workspace(c, T, part, rchunks * align_up((size_t)max_panels, 256), rchunks,
                             max_sims, with_delete != 0);
 }
@@ -2143,6 +2145,7 @@ static int raw_self(dvm_ctx* c, const double* x, const double* z, const double* 
     e.cap = (uint32_t)cap;
     e.chunks = nbody_chunks(e.cap);
     e.rhs_chunks = 1;
+    e.rhs_chunk = kAtChunk;
     e.npad = 256;
     int rc = ensure_workspace(c, cap, (uint64_t)e.chunks * cap, 256, 1, 1, false);
     if (rc) return rc;

@@ -45,6 +45,20 @@ constexpr int kBsST = 256;                     // sources per stage (= sort tile
 constexpr int kAtChunk = 4096;                 // sources per item of the at-target kernels
 constexpr int kCapAlign = 1024;                // capacities are multiples of this
 
+// Sources per work item of a simulation's blob-on-collocation right-hand side:
+// a power of two in [512, kAtChunk], the smallest that still leaves about 600
+// items (four per SM) when the simulation is evaluated alone, so a single
+// simulation fills the GPU.  It depends only on the capacity and the panel
+// count, so the sum is grouped the same way alone and in any batch; a
+// simulation then has at most ~600 chunks, or cap / kAtChunk + 1 when large.
+inline uint32_t rhs_chunk_for(uint32_t cap, int np) {
+    const uint64_t tiles = ((uint64_t)np + 511) / 512;
+    const uint64_t want = ((uint64_t)cap * tiles + 599) / 600;
+    uint32_t c = 512;
+    while (c < (uint32_t)kAtChunk && c < want) c <<= 1;
+    return c;
+}
+
 // Device-side description of one simulation instance.
 struct InstDesc {
     // blob state, SoA, capacity `cap`
@@ -111,10 +125,10 @@ struct InstState {
 struct ListEntry {
     int inst;          // table index
     int chunks;        // N-body source chunks (fixed by capacity)
-    int rhs_chunks;    // at-target source chunks = ceil(cap / kAtChunk)
+    int rhs_chunks;    // at-target source chunks = ceil(cap / rhs_chunk)
     int npad;          // np rounded up to kBsThreads
     uint32_t cap;
-    uint32_t pad;
+    uint32_t rhs_chunk;  // sources per at-target work item (rhs_chunk_for)
     uint64_t coff;     // offset in the concatenated capacity space (multiple of kCapAlign)
     uint64_t poff;     // N-body partials offset (double2): sum chunks * cap
     uint64_t roff;     // at-target partials offset (double2): sum rhs_chunks * npad

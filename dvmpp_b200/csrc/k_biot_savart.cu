@@ -205,27 +205,8 @@ struct StagedTile {
     float2 core[kBsST];
 };
 
-// Reciprocal of both halves on the FMA pipe instead of the MUFU (XU) pipe:
-// the seed 0x7EF311C2 - bits(x) (the constant that minimises the seed's
-// relative error over a binade, 5.1 %, found by a search over that range)
-// and three Newton steps y <- y + y (1 - x y), each two packed FMAs; the
-// result is within 6e-8 relative for every normal x whose reciprocal is
-// normal, on par with one MUFU rcp.approx.  The pair kernel routes one source
-// in sixteen through it: the XU pipe (one reciprocal per pair otherwise)
-// bounds the kernel, the FMA pipe has room for that share.
-__device__ __forceinline__ uint64_t f2rcp_newton(uint64_t x) {
-    const uint32_t lo = 0x7EF311C2u - (uint32_t)x;
-    const uint32_t hi = 0x7EF311C2u - (uint32_t)(x >> 32);
-    uint64_t y = ((uint64_t)hi << 32) | lo;
-    const uint64_t nx = x ^ 0x8000000080000000ull;  // -x, both halves
-    const uint64_t one = 0x3F8000003F800000ull;     // (1, 1)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) y = f2fma(y, f2fma(nx, y, one), y);
-    return y;
-}
-
 // One staged source against the warp's targets (far: no core test).
-template <int WP, bool FMA_RCP = false>
+template <int WP>
 __device__ __forceinline__ void far_pair(uint64_t sx, uint64_t sz, uint64_t sg,
                                          const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                          uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
@@ -234,10 +215,8 @@ __device__ __forceinline__ void far_pair(uint64_t sx, uint64_t sz, uint64_t sg,
         const uint64_t dx = f2sub(tx2[q], sx);
         const uint64_t dz = f2sub(tz2[q], sz);
         const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
-        // one reciprocal per pair, on the XU pipe or (FMA_RCP) the FMA pipe
-        // (padded sources: the reciprocal of ~2e36, Gamma 0)
-        const uint64_t inv = FMA_RCP ? f2rcp_newton(r2)
-                                     : f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
+        // one MUFU reciprocal per pair (padded sources: rcp of ~2e36, Gamma 0)
+        const uint64_t inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
         const uint64_t g = f2mul(inv, sg);
         nu2[q] = f2fma(g, dz, nu2[q]);
         w2[q] = f2fma(g, dx, w2[q]);
@@ -248,29 +227,18 @@ __device__ __forceinline__ void far_pair(uint64_t sx, uint64_t sz, uint64_t sg,
 // (Sharing one reciprocal between the two targets of a packed pair, 1/a = b/(ab),
 // trades one MUFU operation for three FP32 multiplications; it measured 1-4 %
 // slower for 1/8 to 1/2 of the sources, the FMA pipe being nearly as loaded as
-// the MUFU pipe.)
-// The last source of every sixteen takes its reciprocals from the FMA pipe
-// (f2rcp_newton), on both paths, so a pair gets the same bits near or far.
-constexpr int kRcpGroup = 16;
-__device__ __forceinline__ bool fma_rcp_source(int j) { return (j % kRcpGroup) == kRcpGroup - 1; }
-
+// the MUFU pipe.  So did a Newton reciprocal on the FMA pipe for one source in
+// sixteen: 3.5 % slower at N = 2^20.)
 template <int WP>
 __device__ __forceinline__ void stage_far(const StagedTile& __restrict__ src,
                                           const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                           uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
-#pragma unroll 1
-    for (int i0 = 0; i0 < kBsST / 2; i0 += kRcpGroup / 2) {
-#pragma unroll
-        for (int k = 0; k < kRcpGroup / 2; ++k) {  // sources 2 (i0 + k) and 2 (i0 + k) + 1
-            const float4 P = src.pos2[i0 + k];
-            const float4 G = src.gam2[i0 + k];
-            far_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), tx2, tz2, nu2, w2);
-            if (k == kRcpGroup / 2 - 1)
-                far_pair<WP, true>(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), tx2, tz2,
-                                   nu2, w2);
-            else
-                far_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), tx2, tz2, nu2, w2);
-        }
+#pragma unroll 4  // 8 sources per unrolled body
+    for (int i = 0; i < kBsST / 2; ++i) {
+        const float4 P = src.pos2[i];
+        const float4 G = src.gam2[i];
+        far_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), tx2, tz2, nu2, w2);
+        far_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), tx2, tz2, nu2, w2);
     }
 }
 
@@ -308,24 +276,15 @@ __device__ __forceinline__ float core_kernel_expm1(float r2, float rs, float rcp
 // One staged source against the warp's targets with the exact core test.
 template <int WP>
 __device__ __forceinline__ void near_pair(uint64_t sx, uint64_t sz, uint64_t sg, float2 C,
-                                          bool fma_rcp, const uint64_t (&tx2)[WP],
-                                          const uint64_t (&tz2)[WP], uint64_t (&nu2)[WP],
-                                          uint64_t (&w2)[WP]) {
+                                          const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
+                                          uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
 #pragma unroll
     for (int q = 0; q < WP; ++q) {
         const uint64_t dx = f2sub(tx2[q], sx);
         const uint64_t dz = f2sub(tz2[q], sz);
         const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
         const float ra = f2lo(r2), rb = f2hi(r2);
-        float ka, kb;
-        if (fma_rcp) {  // warp-uniform
-            const uint64_t inv = f2rcp_newton(r2);
-            ka = f2lo(inv);
-            kb = f2hi(inv);
-        } else {
-            ka = rcp_approx(ra);
-            kb = rcp_approx(rb);
-        }
+        float ka = rcp_approx(ra), kb = rcp_approx(rb);
         const bool ca = ra < C.x, cb = rb < C.x;
         if (__any_sync(0xffffffffu, ca || cb)) {
             const float qa = core_kernel(ra, C.y, ka), qb = core_kernel(rb, C.y, kb);
@@ -353,10 +312,8 @@ __device__ __forceinline__ void stage_near(const StagedTile& __restrict__ src,
         const float4 P = src.pos2[i];
         const float4 G = src.gam2[i];
         const float2 C0 = src.core[2 * i], C1 = src.core[2 * i + 1];
-        near_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), C0, false, tx2, tz2,
-                  nu2, w2);
-        near_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), C1,
-                  fma_rcp_source(2 * i + 1), tx2, tz2, nu2, w2);
+        near_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), C0, tx2, tz2, nu2, w2);
+        near_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), C1, tx2, tz2, nu2, w2);
     }
 }
 
@@ -591,9 +548,11 @@ __global__ void k_self_combine(const InstDesc* __restrict__ table,
 }
 
 // ---- arbitrary targets --------------------------------------------------------
-// One item = (entry, 256 targets, kAtChunk sources).  Sources are staged with
-// FP64 positions; each pair forms dx, dz in FP64 (exact for close pairs) and,
-// in FP32 mode, evaluates the kernel in FP32 with Kahan-compensated sums.
+// One item = (job, a tile of targets, a chunk of `chunk` sources: kAtChunk for
+// at-target calls, rhs_chunk_for(...) for a simulation's right-hand side).
+// Sources are staged with FP64 positions; each pair forms dx, dz in FP64
+// (exact for close pairs) and, in FP32 mode, evaluates the kernel in FP32 with
+// Kahan-compensated sums.
 struct AtJob {
     const double* tx;
     const double* tz;
@@ -606,6 +565,7 @@ struct AtJob {
     const uint32_t* pns;  // source count on the device, or null -> ns
     uint32_t ns;
     int npad;             // partial row length
+    uint32_t chunk;       // sources per work item (a multiple of 256)
     double2* part;        // [chunk][npad]
     double* circ_part;    // [chunk], or null
 };
@@ -620,7 +580,7 @@ __device__ __forceinline__ void kahan2_fma(uint64_t& s, uint64_t& e, uint64_t a,
     s = t;
 }
 
-// Velocity at targets from a chunk of kAtChunk sources per work item.  FP32
+// Velocity at targets from a chunk of J.chunk sources per work item.  FP32
 // path: 512 targets per item, two per thread; jobs without the close-pair skip
 // (the blob-on-collocation right-hand side) run packed FP32x2 with a per-pair
 // compensated sum (the right-hand side is the small residual normal velocity,
@@ -641,7 +601,7 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
         for (int k = 0; k < njobs; ++k) {
             s_pre[k] = acc;
             const uint32_t ns = jobs[k].pns ? *jobs[k].pns : jobs[k].ns;
-            acc += ((jobs[k].nt + kTile - 1) / kTile) * ((ns + kAtChunk - 1) / kAtChunk);
+            acc += ((jobs[k].nt + kTile - 1) / kTile) * ((ns + jobs[k].chunk - 1) / jobs[k].chunk);
         }
         s_pre[njobs] = acc;
     }
@@ -651,14 +611,14 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
         const int k = locate(s_pre, njobs, item);
         const AtJob J = jobs[k];
         const uint32_t ns = J.pns ? *J.pns : J.ns;
-        const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+        const uint32_t nchunk = (ns + J.chunk - 1) / J.chunk;
         const unsigned local = item - s_pre[k];
         const uint32_t ttile = local / nchunk, c = local % nchunk;
         const uint32_t t0 = ttile * kTile + threadIdx.x, t1 = t0 + 256;  // t1: F32 only
         const double tx0 = t0 < J.nt ? J.tx[t0] : 0.0, tz0 = t0 < J.nt ? J.tz[t0] : 0.0;
         const double tx1 = (F32 && t1 < J.nt) ? J.tx[t1] : 0.0;
         const double tz1 = (F32 && t1 < J.nt) ? J.tz[t1] : 0.0;
-        const uint32_t j0 = c * kAtChunk, j1 = min(ns, j0 + kAtChunk);
+        const uint32_t j0 = c * J.chunk, j1 = min(ns, j0 + J.chunk);
         double uu0 = 0.0, ww0 = 0.0, uu1 = 0.0, ww1 = 0.0, csum = 0.0;
         const uint64_t zero2 = f2pack(0.0f, 0.0f);
         uint64_t snu = zero2, enu = zero2, sw = zero2, ew = zero2;  // -u and w, packed Kahan
@@ -765,7 +725,7 @@ __global__ void k_at_combine(const AtJob* __restrict__ jobs, double* __restrict_
                              double* __restrict__ w) {
     const AtJob J = jobs[0];
     const uint32_t ns = J.pns ? *J.pns : J.ns;
-    const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    const uint32_t nchunk = (ns + J.chunk - 1) / J.chunk;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < J.nt; t += gridDim.x * blockDim.x) {
         double su = 0.0, sw = 0.0;
         for (uint32_t c = 0; c < nchunk; ++c) {
@@ -787,7 +747,7 @@ __global__ void k_rhs_combine(const InstDesc* __restrict__ table, InstState* __r
     const InstDesc& d = table[e.inst];
     const AtJob J = jobs[k];
     const uint32_t ns = st[e.inst].n;
-    const uint32_t nchunk = (ns + kAtChunk - 1) / kAtChunk;
+    const uint32_t nchunk = (ns + J.chunk - 1) / J.chunk;
     for (int i = threadIdx.x; i < d.np; i += blockDim.x) {
         double su = 0.0, sw = 0.0;
         for (uint32_t c = 0; c < nchunk; ++c) {
@@ -825,6 +785,7 @@ __global__ void k_build_rhs_jobs(const InstDesc* __restrict__ table, InstState* 
     J.pns = &st[e.inst].n;
     J.ns = 0;
     J.npad = e.npad;
+    J.chunk = e.rhs_chunk;
     J.part = rhs_part + e.roff;
     J.circ_part = circ_part + e.cofs;
     jobs[k] = J;
@@ -928,6 +889,7 @@ void direct_at_raw(const double* x, const double* z, const double* circ, const d
     J.pns = nullptr;
     J.ns = ns;
     J.npad = (int)std::max<size_t>((nt + 255) / 256 * 256, 256);
+    J.chunk = kAtChunk;
     J.part = part;
     J.circ_part = nullptr;
     cudaMemcpyAsync(job, &J, sizeof(AtJob), cudaMemcpyHostToDevice, s);
@@ -1012,6 +974,7 @@ extern "C" int dvm_biot_savart_at_noalloc(const double* x, const double* z, cons
     J.pns = nullptr;
     J.ns = (uint32_t)ns;
     J.npad = (int)npad;
+    J.chunk = kAtChunk;
     J.part = scratch;  // every entry read by k_at_combine is written by k_at first
     J.circ_part = nullptr;
     AtJob* job = reinterpret_cast<AtJob*>(scratch + (kNoAllocElems - kNoAllocJobElems));
