@@ -21,6 +21,10 @@ influence matrix), a 2^19-blob wake, RK3 dt = 0.002; the FP32-compensated run
 sheet: the FP32 sheet-on-blob velocity alone (ellipse at 20 degrees, wake of
 n blobs); prints its CUDA-event time, pairs/s and FP32 fraction (67 flop/pair).
 
+    python -m dvmpp_b200.cases book [--n 4194304] [--panels 256] [--inside 0.02]
+
+book: the Philox walk, REFLECT and DELETE alone on one simulation (CUDA events).
+
     python -m dvmpp_b200.cases rhs [--n 131072] [--panels 1024] [--reps 3]
 
 rhs: the blob-on-collocation right-hand side alone (same body and wake);
@@ -399,6 +403,47 @@ def run_rhs(n: int, npanels: int, reps: int, seed: int = 2):
             "fp32_peak_frac": tf / _fp32_peak_tflops(sms)}
 
 
+def run_book(n: int, npanels: int, inside: float, reps: int, seed: int = 3):
+    """Bookkeeping phases alone on one simulation: a circle of npanels panels
+    (R = 0.5) and n blobs, a fraction `inside` of them inside the body, the rest
+    in the wake distribution.  CUDA-event time per call of the Philox random
+    walk, REFLECT and DELETE (the blob state is restored between calls), with
+    the algorithmic bytes per blob: walk 32 (read and write x, z), crossing
+    flags 17 (read x, z; a flag), DELETE's move 132 per kept blob (read x, z
+    and the other six arrays, write all eight and the ID)."""
+    ctx = N.Context(0)
+    bx, bz = W.circle(npanels)
+    x, z, g, s = W.wake(n, seed, W.core_size(bx, bz))
+    rng = np.random.default_rng(seed)
+    k = rng.random(n) < inside
+    r = 0.45 * np.sqrt(rng.random(int(k.sum())))
+    th = rng.uniform(0, 2 * np.pi, r.size)
+    x[k], z[k] = r * np.cos(th), r * np.sin(th)
+    out = {"workload": "bookkeeping", "n": n, "panels": npanels, "inside": inside}
+    for name, cross, phase in (("walk_philox", N.REFLECT, N.PHASE_DIFFUSE),
+                               ("reflect", N.REFLECT, N.PHASE_REFLECT),
+                               ("delete", N.DELETE, N.PHASE_DELETE)):
+        sim = ctx.sim(N.Params(capacity=n, rng=N.RNG_PHILOX, surface_cross=cross), bx, bz)
+        ms = []
+        for rep in range(reps + 1):
+            sim.set_blobs(x, z, g, s)
+            ctx.mark(0)
+            sim.phase(phase)
+            ctx.mark(1)
+            if rep:
+                ms.append(ctx.elapsed_ms(0, 1))
+        sim.check()
+        out[name + "_ms"] = float(np.median(ms))
+        if name == "delete":
+            kept = sim.n
+            out["delete_kept"] = kept
+            out["delete_gbs_algorithmic"] = (17.0 * n + 132.0 * kept) / (out[name + "_ms"] / 1e3) / 1e9
+        sim.close()
+    out["walk_gbs_algorithmic"] = 32.0 * n / (out["walk_philox_ms"] / 1e3) / 1e9
+    ctx.close()
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -429,6 +474,11 @@ def main(argv=None):
     sh.add_argument("--n", type=int, default=1 << 17)
     sh.add_argument("--panels", type=int, default=1024)
     sh.add_argument("--reps", type=int, default=3)
+    bk = sub.add_parser("book")
+    bk.add_argument("--n", type=int, default=1 << 22)
+    bk.add_argument("--panels", type=int, default=256)
+    bk.add_argument("--inside", type=float, default=0.02)
+    bk.add_argument("--reps", type=int, default=5)
     rh = sub.add_parser("rhs")
     rh.add_argument("--n", type=int, default=1 << 17)
     rh.add_argument("--panels", type=int, default=1024)
@@ -453,6 +503,8 @@ def main(argv=None):
                                      serial_every=a.serial_every)))
     if a.cmd == "sheet":
         print(json.dumps(run_sheet(a.n, a.panels, a.reps)))
+    if a.cmd == "book":
+        print(json.dumps(run_book(a.n, a.panels, a.inside, a.reps)))
     if a.cmd == "rhs":
         print(json.dumps(run_rhs(a.n, a.panels, a.reps)))
     if a.cmd == "nbody":
