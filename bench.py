@@ -592,7 +592,8 @@ def run_ours(args, dist):
     step_ms_prof = prof["step"][0] / max(prof["step"][1], 1)
     nbody_launch_ms = nb_ms / max(nb_n, 1)
     pairs_per_launch = pairs / max(nb_n, 1)
-    achieved_tflops = 12.0 * pairs_per_launch / (nbody_launch_ms / 1e3) / 1e12
+    achieved_tflops = (12.0 * pairs_per_launch / (nbody_launch_ms / 1e3) / 1e12
+                       if nbody_launch_ms > 0 else 0.0)  # no profiled steps: not measured
     pk = peaks()
     sm_max = float(pk.get("sm_max_mhz", 1965.0))
     fp32_peak = sms * 128 * 2 * sm_max * 1e6 / 1e12
