@@ -614,7 +614,8 @@ def run_ours(args, dist):
     for s in sims:
         s.check()
     plain_ms = dist.max(plain_ms)
-    plain_value = dist.world * args.instances * args.plain_steps / (plain_ms / 1e3)
+    plain_value = (dist.world * args.instances * args.plain_steps / (plain_ms / 1e3)
+                   if args.plain_steps > 0 and plain_ms > 0 else None)
 
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
@@ -717,7 +718,7 @@ def run_ours(args, dist):
                    "l2": "inputs larger than L2 (state + workspace >> 126 MB)",
                    "graph": "one CUDA graph per step, replayed"},
         "plain_gpu": {"value": plain_value, "unit": UNIT, "steps": args.plain_steps,
-                      "ratio_batched_over_plain": value / plain_value,
+                      "ratio_batched_over_plain": value / plain_value if plain_value else None,
                       "how": "each simulation stepped alone (its own launches, no batching)"},
         "roofline": {"bound": "fp32", "kernel": "k_self_f32 (pair kernel)",
                      "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
