@@ -471,7 +471,7 @@ void issue_step(dvm_ctx* c, Plan& pl) {
         prof_end(c, p);
         L += (prec == kF32) ? 4 : 3;
         p = prof_begin(c, DVM_PROF_RHS);
-        sheet_rhs(T, S, sl.d_list, sl.n, prec, ws, sms, s);
+        sheet_rhs(T, S, sl.d_list, sl.n, sl.max_np, prec, ws, sms, s);
         prof_end(c, p);
         L += 3;
     };
@@ -1880,7 +1880,7 @@ int dvm_sim_phase(dvm_sim* s, int phase) {
             break;
         }
         case DVM_PHASE_SOLVE:
-            sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
+            sheet_rhs(T, S, L, 1, np, prec, ws, c->sms, st);
             sheet_solve(T, S, L, 1, np, st);
             break;
         case DVM_PHASE_SHEETBC: sheet_velocity(T, S, L, 1, 0, np, ws, c->sms, st); break;
@@ -1888,7 +1888,7 @@ int dvm_sim_phase(dvm_sim* s, int phase) {
             for (int k = 0; k < (s->h.scheme == kRK3 ? 3 : 1); ++k) {
                 biot_savart_self(T, S, L, 1, prec, ws, c->sms, st,
                                  tuned_config(c, shape_class(s->h.cap, 1)));
-                sheet_rhs(T, S, L, 1, prec, ws, c->sms, st);
+                sheet_rhs(T, S, L, 1, np, prec, ws, c->sms, st);
                 sheet_solve(T, S, L, 1, np, st);
                 sheet_velocity(T, S, L, 1, s->h.scheme == kRK3 ? 2 + k : 1, np, ws, c->sms, st);
             }

@@ -197,7 +197,7 @@ void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* l
                         int precision, const Workspace& ws, int sms, cudaStream_t s);
 // Blob-on-collocation right-hand side b (src/VortexSheet.cpp:171-210).
 void sheet_rhs(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-               int precision, const Workspace& ws, int sms, cudaStream_t s);
+               int max_np, int precision, const Workspace& ws, int sms, cudaStream_t s);
 // Velocity at arbitrary targets from one blob set (src/VelocityKernel.cpp:69-109).
 void direct_at_raw(const double* x, const double* z, const double* circ, const double* sigma,
                    uint32_t ns, const double* tx, const double* tz, uint32_t nt, double* u,

@@ -739,30 +739,59 @@ __global__ void k_at_combine(const AtJob* __restrict__ jobs, double* __restrict_
 }
 
 // b_i = (Ux + u_i) enx_i + (Uz + w_i) enz_i, b_np = -sum(circ)
-// (src/VortexSheet.cpp:206-210); one block per simulation.
-__global__ void k_rhs_combine(const InstDesc* __restrict__ table, InstState* __restrict__ st,
-                              const ListEntry* __restrict__ list, const AtJob* __restrict__ jobs) {
-    const int k = blockIdx.x;
+// (src/VortexSheet.cpp:206-210).  Block (x, k) finishes targets 32x .. 32x+31
+// of simulation k: warp w sums chunks w, w + 8, ... for its lane's target and
+// the eight warp sums are added in warp order; block x = 0 also sums the
+// Kelvin row's circulation partials (thread t takes chunks t, t + 256, ...,
+// then a fixed shuffle tree and the warp sums in order).  The order depends
+// only on the simulation's chunk count, never on the batch.
+__global__ void __launch_bounds__(256) k_rhs_combine(const InstDesc* __restrict__ table,
+                                                     InstState* __restrict__ st,
+                                                     const ListEntry* __restrict__ list,
+                                                     const AtJob* __restrict__ jobs) {
+    __shared__ double s_u[8][32], s_w[8][32], s_c[8];
+    const int k = blockIdx.y;
     const ListEntry e = list[k];
     const InstDesc& d = table[e.inst];
     const AtJob J = jobs[k];
     const uint32_t ns = st[e.inst].n;
     const uint32_t nchunk = (ns + J.chunk - 1) / J.chunk;
-    for (int i = threadIdx.x; i < d.np; i += blockDim.x) {
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * 32 + lane;
+    const bool targets = (int)(blockIdx.x * 32) < d.np;  // block-uniform
+    if (targets) {
         double su = 0.0, sw = 0.0;
-        for (uint32_t c = 0; c < nchunk; ++c) {
-            const double2 v = J.part[(uint64_t)c * J.npad + i];
-            su += v.x;
-            sw += v.y;
+        if (i < d.np)
+            for (uint32_t c = wid; c < nchunk; c += 8) {
+                const double2 v = J.part[(uint64_t)c * J.npad + i];
+                su += v.x;
+                sw += v.y;
+            }
+        s_u[wid][lane] = su;
+        s_w[wid][lane] = sw;
+    }
+    __syncthreads();
+    if (targets && threadIdx.x < 32 && i < d.np) {
+        double su = 0.0, sw = 0.0;
+        for (int q = 0; q < 8; ++q) {
+            su += s_u[q][lane];
+            sw += s_w[q][lane];
         }
         const double ui = dmul(su, kRpi2), wi = dmul(sw, kRpi2);
         d.b[i] = dadd(dmul(dadd(d.ux, ui), d.enx[i]), dmul(dadd(d.uz, wi), d.enz[i]));
     }
-    if (threadIdx.x == 0) {
+    if (blockIdx.x == 0) {  // block-uniform
         double tc = 0.0;
-        for (uint32_t c = 0; c < nchunk; ++c) tc += J.circ_part[c];
-        d.b[d.np] = -tc;
-        st[e.inst].totalcirc = tc;
+        for (uint32_t c = threadIdx.x; c < nchunk; c += 256) tc += J.circ_part[c];
+        for (int o = 16; o > 0; o >>= 1) tc += __shfl_xor_sync(0xffffffffu, tc, o);
+        if (lane == 0) s_c[wid] = tc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0;
+            for (int q = 0; q < 8; ++q) a += s_c[q];
+            d.b[d.np] = -a;
+            st[e.inst].totalcirc = a;
+        }
     }
 }
 
@@ -854,14 +883,14 @@ void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* lis
 }
 
 void sheet_rhs(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
-               int precision, const Workspace& ws, int sms, cudaStream_t s) {
+               int max_np, int precision, const Workspace& ws, int sms, cudaStream_t s) {
     static_assert(sizeof(AtJob) <= 256, "job record size");
     AtJob* jobs = reinterpret_cast<AtJob*>(ws.jobs);
     k_build_rhs_jobs<<<(nlist + 127) / 128, 128, 0, s>>>(table, st, list, nlist, ws.rhs_part,
                                                          ws.circ_part, jobs);
     if (precision == kF32) k_at<true><<<sms * 4, 256, 0, s>>>(jobs, nlist);
     else k_at<false><<<sms * 4, 256, 0, s>>>(jobs, nlist);
-    k_rhs_combine<<<nlist, 256, 0, s>>>(table, st, list, jobs);
+    k_rhs_combine<<<dim3((max_np + 31) / 32, nlist), 256, 0, s>>>(table, st, list, jobs);
 }
 
 size_t direct_at_part_elems(uint32_t ns, uint32_t nt) {

@@ -509,8 +509,15 @@ __device__ __forceinline__ void sheet_sum_f32x2(double xa, double za, double xb,
                                                 const PanelX2* __restrict__ pan, double& ua,
                                                 double& wa, double& ub, double& wb) {
     const uint64_t two = f2pack(2.0f, 2.0f), half = f2pack(0.5f, 0.5f);
+    // Panel terms are summed in FP32 over blocks of eight panels, each block
+    // then added in FP64 (a quarter of the conversions and FP64 adds; the
+    // bench's FP32-vs-FP64 check gave the same worst-case error as per-term FP64
+    // adds).
+    for (int j0 = 0; j0 < np; j0 += 8) {
+        uint64_t ACU = f2pack(0.0f, 0.0f), ACW = f2pack(0.0f, 0.0f);
+        const int jn = min(np, j0 + 8);
 #pragma unroll 2
-    for (int j = 0; j < np; ++j) {
+    for (int j = j0; j < jn; ++j) {
         const PanelX2 P = pan[j];
         const uint64_t CT = P.cs.x, ST = P.cs.y, DS = P.dd.x, IDS = P.dd.y;
         const uint64_t C2T = P.cc.x, S2T = P.cc.y, G0 = P.gd.x, DG = P.gd.y;
@@ -552,10 +559,13 @@ __device__ __forceinline__ void sheet_sum_f32x2(double xa, double za, double xb,
         const uint64_t AY = f2sub(f2mul(HC6, CT), f2mul(C7, ST));
         const uint64_t TU = f2fma(AX, G0, f2mul(QX, DG));
         const uint64_t TW = f2fma(AY, G0, f2mul(QY, DG));
-        ua += (double)f2lo(TU);
-        ub += (double)f2hi(TU);
-        wa += (double)f2lo(TW);
-        wb += (double)f2hi(TW);
+        ACU = f2add(ACU, TU);
+        ACW = f2add(ACW, TW);
+    }
+        ua += (double)f2lo(ACU);
+        ub += (double)f2hi(ACU);
+        wa += (double)f2lo(ACW);
+        wb += (double)f2hi(ACW);
     }
 }
 
