@@ -517,51 +517,51 @@ __device__ __forceinline__ void sheet_sum_f32x2(double xa, double za, double xb,
         uint64_t ACU = f2pack(0.0f, 0.0f), ACW = f2pack(0.0f, 0.0f);
         const int jn = min(np, j0 + 8);
 #pragma unroll 2
-    for (int j = j0; j < jn; ++j) {
-        const PanelX2 P = pan[j];
-        const uint64_t CT = P.cs.x, ST = P.cs.y, DS = P.dd.x, IDS = P.dd.y;
-        const uint64_t C2T = P.cc.x, S2T = P.cc.y, G0 = P.gd.x, DG = P.gd.y;
-        const double xc = sxc[j], zc = szc[j];
-        const uint64_t DX = f2pack((float)(xa - xc), (float)(xb - xc));
-        const uint64_t DZ = f2pack((float)(za - zc), (float)(zb - zc));
-        const uint64_t C1 = f2sub(f2pack(0.0f, 0.0f), f2fma(DX, CT, f2mul(DZ, ST)));
-        const uint64_t R2 = f2fma(DX, DX, f2mul(DZ, DZ));
-        const uint64_t C5 = f2sub(f2mul(DX, ST), f2mul(DZ, CT));
-        const float r2a = f2lo(R2), r2b = f2hi(R2);
-        const uint64_t XX =
-            f2mul(f2mul(DS, f2fma(two, C1, DS)), f2pack(rcp_approx(r2a), rcp_approx(r2b)));
-        const uint64_t Y = f2mul(C5, DS);
-        const uint64_t X = f2fma(C1, DS, R2);
-        const float Xa = f2lo(X), Xb = f2hi(X);
-        const uint64_t T = f2mul(Y, f2pack(rcp_approx(Xa), rcp_approx(Xb)));
-        const float xxa = f2lo(XX), xxb = f2hi(XX), ta = f2lo(T), tb = f2hi(T);
-        const bool nla = !(fabsf(xxa) <= 0.25f), nlb = !(fabsf(xxb) <= 0.25f);
-        const bool wa_ = !(Xa > 0.0f && fabsf(ta) <= 0.25f), wb_ = !(Xb > 0.0f && fabsf(tb) <= 0.25f);
-        uint64_t C6 = f2log1p_quarter(XX);
-        uint64_t C7 = f2atan_quarter(T);
-        if (__any_sync(0xffffffffu, nla || nlb || wa_ || wb_)) {
-            float c6a = f2lo(C6), c6b = f2hi(C6), c7a = f2lo(C7), c7b = f2hi(C7);
-            const double ex = sex[j], ez = sez[j];
-            near_values(xa, za, ex, ez, xxa, r2a, f2lo(Y), Xa, nla, wa_, c6a, c7a);
-            near_values(xb, zb, ex, ez, xxb, r2b, f2hi(Y), Xb, nlb, wb_, c6b, c7b);
-            C6 = f2pack(c6a, c6b);
-            C7 = f2pack(c7a, c7b);
+        for (int j = j0; j < jn; ++j) {
+            const PanelX2 P = pan[j];
+            const uint64_t CT = P.cs.x, ST = P.cs.y, DS = P.dd.x, IDS = P.dd.y;
+            const uint64_t C2T = P.cc.x, S2T = P.cc.y, G0 = P.gd.x, DG = P.gd.y;
+            const double xc = sxc[j], zc = szc[j];
+            const uint64_t DX = f2pack((float)(xa - xc), (float)(xb - xc));
+            const uint64_t DZ = f2pack((float)(za - zc), (float)(zb - zc));
+            const uint64_t C1 = f2sub(f2pack(0.0f, 0.0f), f2fma(DX, CT, f2mul(DZ, ST)));
+            const uint64_t R2 = f2fma(DX, DX, f2mul(DZ, DZ));
+            const uint64_t C5 = f2sub(f2mul(DX, ST), f2mul(DZ, CT));
+            const float r2a = f2lo(R2), r2b = f2hi(R2);
+            const uint64_t XX =
+                f2mul(f2mul(DS, f2fma(two, C1, DS)), f2pack(rcp_approx(r2a), rcp_approx(r2b)));
+            const uint64_t Y = f2mul(C5, DS);
+            const uint64_t X = f2fma(C1, DS, R2);
+            const float Xa = f2lo(X), Xb = f2hi(X);
+            const uint64_t T = f2mul(Y, f2pack(rcp_approx(Xa), rcp_approx(Xb)));
+            const float xxa = f2lo(XX), xxb = f2hi(XX), ta = f2lo(T), tb = f2hi(T);
+            const bool nla = !(fabsf(xxa) <= 0.25f), nlb = !(fabsf(xxb) <= 0.25f);
+            const bool wa_ = !(Xa > 0.0f && fabsf(ta) <= 0.25f), wb_ = !(Xb > 0.0f && fabsf(tb) <= 0.25f);
+            uint64_t C6 = f2log1p_quarter(XX);
+            uint64_t C7 = f2atan_quarter(T);
+            if (__any_sync(0xffffffffu, nla || nlb || wa_ || wb_)) {
+                float c6a = f2lo(C6), c6b = f2hi(C6), c7a = f2lo(C7), c7b = f2hi(C7);
+                const double ex = sex[j], ez = sez[j];
+                near_values(xa, za, ex, ez, xxa, r2a, f2lo(Y), Xa, nla, wa_, c6a, c7a);
+                near_values(xb, zb, ex, ez, xxb, r2b, f2hi(Y), Xb, nlb, wb_, c6b, c7b);
+                C6 = f2pack(c6a, c6b);
+                C7 = f2pack(c7a, c7b);
+            }
+            const uint64_t C8 = f2fma(DX, S2T, f2mul(DZ, C2T));
+            const uint64_t C9 = f2sub(f2mul(DX, C2T), f2mul(DZ, S2T));
+            const uint64_t HC6 = f2mul(half, C6);
+            const uint64_t H6 = f2mul(HC6, IDS), C7I = f2mul(C7, IDS);
+            // qx = -st + c8 h6 + (c1 ct + c5 st) c7i;  qy = ct + c9 h6 + (c1 st - c5 ct) c7i
+            const uint64_t QX = f2fma(f2fma(C1, CT, f2mul(C5, ST)), C7I, f2fma(C8, H6, f2sub(f2pack(0.0f, 0.0f), ST)));
+            const uint64_t QY = f2fma(f2sub(f2mul(C1, ST), f2mul(C5, CT)), C7I, f2fma(C9, H6, CT));
+            // px + qx = -c6/2 sin - c7 cos;  py + qy = c6/2 cos - c7 sin
+            const uint64_t AX = f2sub(f2pack(0.0f, 0.0f), f2fma(HC6, ST, f2mul(C7, CT)));
+            const uint64_t AY = f2sub(f2mul(HC6, CT), f2mul(C7, ST));
+            const uint64_t TU = f2fma(AX, G0, f2mul(QX, DG));
+            const uint64_t TW = f2fma(AY, G0, f2mul(QY, DG));
+            ACU = f2add(ACU, TU);
+            ACW = f2add(ACW, TW);
         }
-        const uint64_t C8 = f2fma(DX, S2T, f2mul(DZ, C2T));
-        const uint64_t C9 = f2sub(f2mul(DX, C2T), f2mul(DZ, S2T));
-        const uint64_t HC6 = f2mul(half, C6);
-        const uint64_t H6 = f2mul(HC6, IDS), C7I = f2mul(C7, IDS);
-        // qx = -st + c8 h6 + (c1 ct + c5 st) c7i;  qy = ct + c9 h6 + (c1 st - c5 ct) c7i
-        const uint64_t QX = f2fma(f2fma(C1, CT, f2mul(C5, ST)), C7I, f2fma(C8, H6, f2sub(f2pack(0.0f, 0.0f), ST)));
-        const uint64_t QY = f2fma(f2sub(f2mul(C1, ST), f2mul(C5, CT)), C7I, f2fma(C9, H6, CT));
-        // px + qx = -c6/2 sin - c7 cos;  py + qy = c6/2 cos - c7 sin
-        const uint64_t AX = f2sub(f2pack(0.0f, 0.0f), f2fma(HC6, ST, f2mul(C7, CT)));
-        const uint64_t AY = f2sub(f2mul(HC6, CT), f2mul(C7, ST));
-        const uint64_t TU = f2fma(AX, G0, f2mul(QX, DG));
-        const uint64_t TW = f2fma(AY, G0, f2mul(QY, DG));
-        ACU = f2add(ACU, TU);
-        ACW = f2add(ACW, TW);
-    }
         ua += (double)f2lo(ACU);
         ub += (double)f2hi(ACU);
         wa += (double)f2lo(ACW);
