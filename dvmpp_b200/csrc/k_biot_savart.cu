@@ -580,28 +580,48 @@ __device__ __forceinline__ void kahan2_fma(uint64_t& s, uint64_t& e, uint64_t a,
     s = t;
 }
 
-// Velocity at targets from a chunk of J.chunk sources per work item.  FP32
-// path: 512 targets per item, two per thread; jobs without the close-pair skip
-// (the blob-on-collocation right-hand side) run packed FP32x2 with a per-pair
-// compensated sum (the right-hand side is the small residual normal velocity,
-// so its rounding must stay relative to the few large near-blob terms, not
-// compound) and the core kernel, when any lane of the warp has a pair inside
-// a core, for both halves with a select; the skip jobs (at-target plugin
-// calls, probes) run the scalar loop.  FP64 path: 256 targets per item, the
-// reference's operation order.
+// Velocity at targets from a chunk of J.chunk sources per work item, 256
+// targets per item, one per thread.
+//
+// FP32 jobs without the close-pair skip (the blob-on-collocation right-hand
+// side) pack two SOURCES per FP32x2 instruction, so no lane idles however few
+// targets a body has.  Offsets are formed without per-pair conversions: every
+// position is taken relative to the job's first target in FP64 and split
+// exactly into an FP32 pair (hi, lo = the FP64 remainder); dx = (t_hi - s_hi)
+// + (t_lo - s_lo), exact before its final rounding for close pairs (Sterbenz)
+// and within an ulp otherwise.  Each pair keeps its compensated update (the
+// right-hand side is the small residual normal velocity, so its rounding must
+// stay relative to the few large near-blob terms, not compound): one Kahan
+// sum per half, the halves added at the end.  The core kernel runs for both
+// halves when any lane of the warp has a pair inside a core.  Sources are
+// staged as packed pairs (two 16-byte loads bring positions, two more the
+// circulations and core constants).  Skip jobs (at-target plugin calls,
+// probes) and FP64 jobs run the scalar loops.
+struct AtStage {
+    float4 pos_hi[128];  // (x_hi a, x_hi b, z_hi a, z_hi b) of sources 2i, 2i+1
+    float4 pos_lo[128];  // (x_lo a, x_lo b, z_lo a, z_lo b)
+    float4 cst[128];     // (circ a, circ b, 10 sigma^2 a, 10 sigma^2 b)
+    float2 rs[128];      // (1/sigma^2 a, 1/sigma^2 b)
+};
+
+__device__ __forceinline__ void split_hi_lo(double v, float& hi, float& lo) {
+    hi = (float)v;
+    lo = (float)(v - (double)hi);
+}
+
 template <bool F32>
 __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int njobs) {
-    constexpr uint32_t kTile = F32 ? 512 : 256;
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ double s_x[256], s_z[256], s_c[256], s_thr[256], s_rs[256];
-    __shared__ float s_cf[256], s_thrf[256], s_rsf[256];  // FP32 copies (F32 path)
+    __shared__ float s_cf[256], s_thrf[256], s_rsf[256];  // FP32 copies (scalar FP32 path)
+    __shared__ AtStage s_pk;                               // packed pairs (fast FP32 path)
     __shared__ double s_red[8];
     if (threadIdx.x == 0) {
         unsigned acc = 0;
         for (int k = 0; k < njobs; ++k) {
             s_pre[k] = acc;
             const uint32_t ns = jobs[k].pns ? *jobs[k].pns : jobs[k].ns;
-            acc += ((jobs[k].nt + kTile - 1) / kTile) * ((ns + jobs[k].chunk - 1) / jobs[k].chunk);
+            acc += ((jobs[k].nt + 255) / 256) * ((ns + jobs[k].chunk - 1) / jobs[k].chunk);
         }
         s_pre[njobs] = acc;
     }
@@ -610,23 +630,54 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
     for (unsigned item = blockIdx.x; item < total; item += gridDim.x) {
         const int k = locate(s_pre, njobs, item);
         const AtJob J = jobs[k];
+        const bool packed = F32 && !J.skip_close;
         const uint32_t ns = J.pns ? *J.pns : J.ns;
         const uint32_t nchunk = (ns + J.chunk - 1) / J.chunk;
         const unsigned local = item - s_pre[k];
         const uint32_t ttile = local / nchunk, c = local % nchunk;
-        const uint32_t t0 = ttile * kTile + threadIdx.x, t1 = t0 + 256;  // t1: F32 only
-        const double tx0 = t0 < J.nt ? J.tx[t0] : 0.0, tz0 = t0 < J.nt ? J.tz[t0] : 0.0;
-        const double tx1 = (F32 && t1 < J.nt) ? J.tx[t1] : 0.0;
-        const double tz1 = (F32 && t1 < J.nt) ? J.tz[t1] : 0.0;
+        const uint32_t t = ttile * 256 + threadIdx.x;
+        const double tx = t < J.nt ? J.tx[t] : 0.0, tz = t < J.nt ? J.tz[t] : 0.0;
+        const double ox = J.tx[0], oz = J.tz[0];  // the job's origin: its first target
+        float txh, txl, tzh, tzl;
+        split_hi_lo(tx - ox, txh, txl);
+        split_hi_lo(tz - oz, tzh, tzl);
+        const uint64_t TXH = f2pack(txh, txh), TXL = f2pack(txl, txl);
+        const uint64_t TZH = f2pack(tzh, tzh), TZL = f2pack(tzl, tzl);
         const uint32_t j0 = c * J.chunk, j1 = min(ns, j0 + J.chunk);
-        double uu0 = 0.0, ww0 = 0.0, uu1 = 0.0, ww1 = 0.0, csum = 0.0;
+        double uu = 0.0, ww = 0.0, csum = 0.0;
         const uint64_t zero2 = f2pack(0.0f, 0.0f);
         uint64_t snu = zero2, enu = zero2, sw = zero2, ew = zero2;  // -u and w, packed Kahan
-        float su[2] = {0.f, 0.f}, cu[2] = {0.f, 0.f}, sws[2] = {0.f, 0.f}, cws[2] = {0.f, 0.f};
+        float su = 0.f, cu = 0.f, sws = 0.f, cws = 0.f;
         for (uint32_t s0 = j0; s0 < j1; s0 += 256) {
             __syncthreads();
             const uint32_t j = s0 + threadIdx.x;
-            if (j < j1) {
+            if (packed) {
+                // slot (pair i = tid / 2, half h = tid % 2); a slot past the
+                // chunk holds a far, circulation-free source (it adds 0)
+                float xh = 1.0e18f, xl = 0.f, zh = 0.f, zl = 0.f, cf = 0.f, thr = 0.f, rsf = 0.f;
+                if (j < j1) {
+                    const double sg = J.ss[j];
+                    const double s2 = dmul(sg, sg);
+                    split_hi_lo(J.sx[j] - ox, xh, xl);
+                    split_hi_lo(J.sz[j] - oz, zh, zl);
+                    cf = (float)J.sc[j];
+                    thr = (float)dmul(10.0, s2);
+                    rsf = (float)ddiv(1.0, s2);
+                    if (ttile == 0) csum += J.sc[j];
+                }
+                const int i = threadIdx.x >> 1, h = threadIdx.x & 1;
+                float* ph = reinterpret_cast<float*>(&s_pk.pos_hi[i]);
+                float* pl = reinterpret_cast<float*>(&s_pk.pos_lo[i]);
+                float* pc = reinterpret_cast<float*>(&s_pk.cst[i]);
+                float* pr = reinterpret_cast<float*>(&s_pk.rs[i]);
+                ph[h] = xh;
+                ph[2 + h] = zh;
+                pl[h] = xl;
+                pl[2 + h] = zl;
+                pc[h] = cf;
+                pc[2 + h] = thr;
+                pr[h] = rsf;
+            } else if (j < j1) {
                 const double sg = J.ss[j];
                 const double s2 = dmul(sg, sg);
                 s_x[threadIdx.x] = J.sx[j];
@@ -643,71 +694,62 @@ __global__ void __launch_bounds__(256) k_at(const AtJob* __restrict__ jobs, int 
             }
             __syncthreads();
             const int cnt = (int)min(256u, j1 - s0);
-            if (F32 && !J.skip_close) {
-                for (int jj = 0; jj < cnt; ++jj) {
-                    const double sx = s_x[jj], sz = s_z[jj];
-                    const uint64_t DX = f2pack((float)(tx0 - sx), (float)(tx1 - sx));
-                    const uint64_t DZ = f2pack((float)(tz0 - sz), (float)(tz1 - sz));
+            if (packed) {
+                for (int i = 0; i < (cnt + 1) / 2; ++i) {
+                    const float4 H = s_pk.pos_hi[i], L = s_pk.pos_lo[i], Cs = s_pk.cst[i];
+                    const uint64_t DX = f2add(f2sub(TXH, f2pack(H.x, H.y)),
+                                              f2sub(TXL, f2pack(L.x, L.y)));
+                    const uint64_t DZ = f2add(f2sub(TZH, f2pack(H.z, H.w)),
+                                              f2sub(TZL, f2pack(L.z, L.w)));
                     const uint64_t R2 = f2fma(DX, DX, f2mul(DZ, DZ));
-                    const float ra = f2lo(R2), rb = f2hi(R2), thr = s_thrf[jj];
+                    const float ra = f2lo(R2), rb = f2hi(R2);
                     float ka = rcp_approx(ra), kb = rcp_approx(rb);
-                    const bool ca = ra < thr, cb = rb < thr;
+                    const bool ca = ra < Cs.z, cb = rb < Cs.w;
                     if (__any_sync(0xffffffffu, ca || cb)) {
-                        const float rs = s_rsf[jj];
-                        const float qa = core_kernel_expm1(ra, rs, ka);
-                        const float qb = core_kernel_expm1(rb, rs, kb);
+                        const float2 R = s_pk.rs[i];
+                        const float qa = core_kernel_expm1(ra, R.x, ka);
+                        const float qb = core_kernel_expm1(rb, R.y, kb);
                         ka = ca ? qa : ka;
                         kb = cb ? qb : kb;
                     }
-                    const float cf = s_cf[jj];
-                    const uint64_t G = f2mul(f2pack(ka, kb), f2pack(cf, cf));
+                    const uint64_t G = f2mul(f2pack(ka, kb), f2pack(Cs.x, Cs.y));
                     kahan2_fma(snu, enu, G, DZ);
                     kahan2_fma(sw, ew, G, DX);
                 }
             } else if (F32) {
-                for (int h = 0; h < 2; ++h) {
-                    const double tx = h ? tx1 : tx0, tz = h ? tz1 : tz0;
-                    for (int jj = 0; jj < cnt; ++jj) {
-                        const float dx = (float)(tx - s_x[jj]);
-                        const float dz = (float)(tz - s_z[jj]);
-                        const float r2 = fmaf(dx, dx, dz * dz);
-                        if (!(r2 > 1e-15f)) continue;  // skip_close (computeInducedAt :89)
-                        float K = rcp_approx(r2);
-                        if (r2 < s_thrf[jj]) K = core_kernel_expm1(r2, s_rsf[jj], K);
-                        const float g = K * s_cf[jj];
-                        kahan(su[h], cu[h], -g * dz);
-                        kahan(sws[h], cws[h], g * dx);
-                    }
+                for (int jj = 0; jj < cnt; ++jj) {
+                    const float dx = (float)(tx - s_x[jj]);
+                    const float dz = (float)(tz - s_z[jj]);
+                    const float r2 = fmaf(dx, dx, dz * dz);
+                    if (!(r2 > 1e-15f)) continue;  // skip_close (computeInducedAt :89)
+                    float K = rcp_approx(r2);
+                    if (r2 < s_thrf[jj]) K = core_kernel_expm1(r2, s_rsf[jj], K);
+                    const float g = K * s_cf[jj];
+                    kahan(su, cu, -g * dz);
+                    kahan(sws, cws, g * dx);
                 }
             } else {
                 for (int jj = 0; jj < cnt; ++jj) {
-                    const double dx = dsub(tx0, s_x[jj]);
-                    const double dz = dsub(tz0, s_z[jj]);
+                    const double dx = dsub(tx, s_x[jj]);
+                    const double dz = dsub(tz, s_z[jj]);
                     const double r2 = dadd(dmul(dx, dx), dmul(dz, dz));
                     if (J.skip_close && !(r2 > 1e-15)) continue;
                     double K;
                     if (r2 < s_thr[jj]) K = ddiv(dsub(1.0, exp(dmul(-r2, s_rs[jj]))), r2);
                     else K = __drcp_rn(r2);  // correctly rounded: the same value as 1.0 / r2
-                    uu0 = dsub(uu0, dmul(dmul(K, dz), s_c[jj]));
-                    ww0 = dadd(ww0, dmul(dmul(K, dx), s_c[jj]));
+                    uu = dsub(uu, dmul(dmul(K, dz), s_c[jj]));
+                    ww = dadd(ww, dmul(dmul(K, dx), s_c[jj]));
                 }
             }
         }
-        if (F32) {
-            if (!J.skip_close) {
-                uu0 = -((double)f2lo(snu) + (double)f2lo(enu));
-                uu1 = -((double)f2hi(snu) + (double)f2hi(enu));
-                ww0 = (double)f2lo(sw) + (double)f2lo(ew);
-                ww1 = (double)f2hi(sw) + (double)f2hi(ew);
-            } else {
-                uu0 = (double)su[0] - (double)cu[0];
-                ww0 = (double)sws[0] - (double)cws[0];
-                uu1 = (double)su[1] - (double)cu[1];
-                ww1 = (double)sws[1] - (double)cws[1];
-            }
-            if (t1 < J.nt) J.part[(uint64_t)c * J.npad + t1] = make_double2(uu1, ww1);
+        if (packed) {
+            uu = -(((double)f2lo(snu) + (double)f2lo(enu)) + ((double)f2hi(snu) + (double)f2hi(enu)));
+            ww = ((double)f2lo(sw) + (double)f2lo(ew)) + ((double)f2hi(sw) + (double)f2hi(ew));
+        } else if (F32) {
+            uu = (double)su - (double)cu;
+            ww = (double)sws - (double)cws;
         }
-        if (t0 < J.nt) J.part[(uint64_t)c * J.npad + t0] = make_double2(uu0, ww0);
+        if (t < J.nt) J.part[(uint64_t)c * J.npad + t] = make_double2(uu, ww);
         if (ttile == 0 && J.circ_part) {
             for (int o = 16; o > 0; o >>= 1) csum += __shfl_xor_sync(0xffffffffu, csum, o);
             if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = csum;
