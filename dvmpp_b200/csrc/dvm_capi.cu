@@ -48,7 +48,6 @@ namespace {
             return fail(DVM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-constexpr int kTableCap = 4096;
 constexpr size_t kMaxPlans = 32;       // cached batch plans per context (LRU)
 constexpr size_t kPoolPerPlan = 6144;  // list entries per plan: 4 partitions + 1 reordered
                                        // pair-kernel list, x 1024 sims
@@ -104,8 +103,8 @@ std::vector<ListEntry> costliest_first(const std::vector<ListEntry>& h) {
 }
 
 bool valid_pair_config(const dvm_pair_config& p) {
-    if (p.tile != 256 && p.tile != 128) return false;
-    if (p.ctas_per_sm < 1 || p.ctas_per_sm > (p.tile == 128 ? 4 : 3)) return false;
+    if (p.tile != 256) return false;
+    if (p.ctas_per_sm < 1 || p.ctas_per_sm > 3) return false;
     return p.order == 0 || p.order == 1;
 }
 
@@ -342,6 +341,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     const size_t o_keys_in = take(8 * cap), o_keys_out = take(8 * cap), o_vals = take(4 * cap),
                  o_perm = take(4 * cap), o_packed = take(32 * cap),
                  o_meta = take(sizeof(TileMeta) * (cap / kBsST + 1)), o_part = take(16 * part),
+                 o_macc = take(16 * cap), o_mexp = take(sizeof(int) * 2 * kTableCap),
                  o_rhs = take(16 * rhs), o_circ = take(8 * circ + 8), o_cub = take(cub + 256),
                  o_work = take(64 * sizeof(unsigned)), o_flags = take(cap),
                  o_tiles = take(4 * (cap / 1024 + 1)),
@@ -368,6 +368,8 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     w.packed_cap = cap;
     w.meta = reinterpret_cast<TileMeta*>(b + o_meta);
     w.part = reinterpret_cast<double2*>(b + o_part);
+    w.macc = reinterpret_cast<unsigned long long*>(b + o_macc);
+    w.mexp = reinterpret_cast<int*>(b + o_mexp);
     w.rhs_part = reinterpret_cast<double2*>(b + o_rhs);
     w.circ_part = reinterpret_cast<double*>(b + o_circ);
     w.cub_tmp = b + o_cub;
@@ -1920,7 +1922,7 @@ int dvm_sim_step(dvm_sim* s, int nsteps) {
 int dvm_step_batch(dvm_ctx* c, dvm_sim* const* sims, int nsims, int nsteps, int use_graph) {
     if (!c || (nsims && !sims) || nsims < 0 || nsteps < 0) return fail(DVM_ERR_ARG, "bad argument");
     if (nsims == 0 || nsteps == 0) return DVM_OK;
-    if (nsims > 1024) return fail(DVM_ERR_ARG, "at most 1024 simulations per batch");
+    if (nsims > dvmk::kMaxBatch) return fail(DVM_ERR_ARG, "at most 1024 simulations per batch");
     std::lock_guard<std::mutex> lk(c->mu);
     CK(cudaSetDevice(c->device));
     std::vector<int> slots(nsims);
@@ -1935,8 +1937,7 @@ int dvm_step_batch(dvm_ctx* c, dvm_sim* const* sims, int nsims, int nsteps, int 
 namespace {
 const dvm_pair_config kCandidates[] = {
     {256, 3, 0, 0}, {256, 2, 0, 0}, {256, 1, 0, 0}, {256, 3, 1, 0}, {256, 2, 1, 0},
-    {256, 1, 1, 0}, {128, 4, 0, 0}, {128, 3, 0, 0}, {128, 2, 0, 0}, {128, 1, 0, 0},
-    {128, 4, 1, 0}, {128, 3, 1, 0}, {128, 2, 1, 0}, {128, 1, 1, 0}};
+    {256, 1, 1, 0}};
 constexpr int kNumCandidates = (int)(sizeof(kCandidates) / sizeof(kCandidates[0]));
 static_assert(kNumCandidates <= DVM_TUNE_MAX_CANDIDATES, "candidate table too long");
 
@@ -2060,9 +2061,8 @@ int dvm_ctx_autotune(dvm_ctx* c, dvm_sim* const* sims, int nsims, int reps, dvm_
                             c->sms, c->stream, to_internal(p));
     };
     int err = DVM_OK;
-    // one untimed launch of each kernel variant (module load, caches)
+    // one untimed launch (module load, caches)
     launch(kCandidates[0]);
-    launch(kCandidates[6]);
     std::memset(out, 0, sizeof(*out));
     out->shape_class = shape_class(total, (int)slots.size());
     out->candidates = kNumCandidates;
@@ -2090,7 +2090,7 @@ int dvm_ctx_autotune(dvm_ctx* c, dvm_sim* const* sims, int nsims, int reps, dvm_
     cudaEventDestroy(b);
     if (err) return err;
     CK(cudaGetLastError());
-    g_launches += 4 + (uint64_t)kNumCandidates * reps;  // keys + pack, 2 warm-ups, the timed ones
+    g_launches += 3 + (uint64_t)kNumCandidates * reps;  // keys + pack, the warm-up, the timed ones
     out->best = kCandidates[best];
     out->best_ms = out->ms[best];
     out->default_ms = out->ms[0];

@@ -44,6 +44,8 @@ constexpr int kBsTT = kBsThreads * kBsR;       // 1024 targets per item
 constexpr int kBsST = 256;                     // sources per stage (= sort tile)
 constexpr int kAtChunk = 4096;                 // sources per item of the at-target kernels
 constexpr int kCapAlign = 1024;                // capacities are multiples of this
+constexpr int kMaxBatch = 1024;                // simulations per batched step
+constexpr int kTableCap = 4096;                // simulation slots per context
 
 // Sources per work item of a simulation's blob-on-collocation right-hand side:
 // a power of two in [512, kAtChunk], the smallest that still leaves about 600
@@ -152,6 +154,12 @@ struct Workspace {
     uint64_t packed_cap = 0;       // slots of `packed`
     TileMeta* meta = nullptr;      // total_cap / kBsST
     double2* part = nullptr;       // N-body partials
+    // FP32 N-body, mutual far tiles: per sorted blob two 64-bit fixed-point sums
+    // (Gamma_i K dz, Gamma_i K dx over the targets i whose tile evaluated this blob as a
+    // source), 2 * total_cap; and per simulation slot the two exponent bounds of
+    // their scale (2 * kTableCap)
+    unsigned long long* macc = nullptr;
+    int* mexp = nullptr;
     double2* rhs_part = nullptr;   // at-target partials
     double* circ_part = nullptr;
     void* cub_tmp = nullptr;

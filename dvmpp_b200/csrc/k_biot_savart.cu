@@ -36,7 +36,7 @@
 namespace dvmk {
 namespace {
 
-constexpr int kMaxList = 1024;  // simulations per batched launch
+constexpr int kMaxList = kMaxBatch;  // simulations per batched launch
 
 __device__ __forceinline__ uint32_t spread16(uint32_t v) {
     v &= 0xFFFFu;
@@ -92,9 +92,10 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
                                                 double4* __restrict__ packed,
                                                 double2* __restrict__ pxz,
                                                 float4* __restrict__ pf,
-                                                TileMeta* __restrict__ meta) {
+                                                TileMeta* __restrict__ meta,
+                                                int* __restrict__ mexp) {
     __shared__ unsigned s_pre[kMaxList + 1];
-    __shared__ double s_red[5][kBsST / 32];
+    __shared__ double s_red[7][kBsST / 32];
     if (threadIdx.x == 0) {
         unsigned acc = 0;
         for (int k = 0; k < nlist; ++k) {
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
         const uint32_t n = st[e.inst].n;
         const uint32_t i = (item - s_pre[k]) * kBsST + threadIdx.x;
         double xmin = DBL_MAX, xmax = -DBL_MAX, zmin = DBL_MAX, zmax = -DBL_MAX, thr = 0.0;
+        double gmax = 0.0, tmin = DBL_MAX;  // max |Gamma| (as the FP32 path rounds it), min 10 sigma^2
         if (i < n) {
             const uint32_t p = perm ? perm[e.coff + i] : i;
             const double4 v = make_double4(d.x[p], d.z[p], d.circ[p], d.sigma[p]);
@@ -124,7 +126,8 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
             }
             xmin = xmax = v.x;
             zmin = zmax = v.y;
-            thr = 10.0 * (v.w * v.w);
+            thr = tmin = 10.0 * (v.w * v.w);
+            gmax = fabs((double)(float)v.z);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -133,6 +136,8 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
             zmin = fmin(zmin, __shfl_xor_sync(0xffffffffu, zmin, o));
             zmax = fmax(zmax, __shfl_xor_sync(0xffffffffu, zmax, o));
             thr = fmax(thr, __shfl_xor_sync(0xffffffffu, thr, o));
+            gmax = fmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+            tmin = fmin(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
         }
         const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
         if (lane == 0) {
@@ -141,6 +146,8 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
             s_red[2][wid] = zmin;
             s_red[3][wid] = zmax;
             s_red[4][wid] = thr;
+            s_red[5][wid] = gmax;
+            s_red[6][wid] = tmin;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -159,6 +166,17 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
             }
             m.pad0 = m.pad1 = m.pad2 = 0.0;
             meta[(e.coff + (uint64_t)(item - s_pre[k]) * kBsST) / kBsST] = m;
+            if (mexp) {  // exponent bounds of the simulation's mutual sums (order-free max)
+                double gm = s_red[5][0], tm = s_red[6][0];
+                for (int q = 1; q < kBsST / 32; ++q) {
+                    gm = fmax(gm, s_red[5][q]);
+                    tm = fmin(tm, s_red[6][q]);
+                }
+                const int eg = gm > 0.0 ? ilogb(gm) + 1 : -1100;  // max |Gamma| < 2^eg
+                const int es = (1 - ilogb(fmax(tm, 1e-30))) >> 1;  // 1 / sqrt(min) <= 2^es
+                atomicMax(&mexp[2 * e.inst], eg);
+                atomicMax(&mexp[2 * e.inst + 1], es);
+            }
         }
         __syncthreads();
     }
@@ -183,16 +201,23 @@ __device__ __forceinline__ uint32_t chunk_size(uint32_t n, int chunks) {
 }
 
 // ---- FP32 pair loops --------------------------------------------------------
-// A work item belongs to ONE warp: 256 consecutive sorted targets (8 per lane)
-// against one source chunk.  The warp stages its own source tiles in shared
-// memory and never waits for other warps, so far-path and near-path warps of a
-// block do not hold each other up at barriers.
-// Work-item shape: WR consecutive sorted targets per lane (WR / 2 packed
-// FP32x2 target pairs), 32 * WR targets per warp item.  WR is 8 (256-target
-// items) or 4 (128-target items); the choice changes which targets share a
-// warp, never a target's own operation sequence, so results do not depend on it.
+// A work item belongs to ONE warp: one 256-blob sort tile of targets (8
+// consecutive ones per lane, 4 packed FP32x2 target pairs) against one source
+// chunk.  The warp stages its own source tiles in shared memory and never waits
+// for other warps, so far-path and near-path warps of a block do not hold each
+// other up at barriers.
+//
+// Tile pairs.  A (target tile a, source tile b) stage is
+//   mutual far  when the two tiles' boxes are farther apart than both tiles'
+//               core radii (every pair, either way round, has K = 1/r2): the
+//               item of the lower tile evaluates it once for both directions
+//               and the item of the upper tile skips it;
+//   far         when only the source cores are out of reach (no core test);
+//   near        otherwise (the exact core test per pair; a == b is near).
 constexpr int kWWarps = 4;            // independent warps per block
-constexpr int kSelfMinBlocks = 3;     // blocks per SM the 256-target variant's registers allow
+constexpr int kSelfMinBlocks = 3;     // blocks per SM the registers allow
+constexpr int kWR = 8;                // targets per lane
+constexpr int kWP = kWR / 2;          // packed target pairs per lane
 
 // A warp's staged source tile: pos2[i] = (x, z) of sources 2i and 2i+1 (FP32
 // offsets), gam2[i] = (Gamma, Gamma) of both, core[j] = (10 sigma^2,
@@ -239,6 +264,93 @@ __device__ __forceinline__ void stage_far(const StagedTile& __restrict__ src,
         const float4 G = src.gam2[i];
         far_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), tx2, tz2, nu2, w2);
         far_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), tx2, tz2, nu2, w2);
+    }
+}
+
+// Mutual far pairs: one reciprocal per pair serves both directions.  Besides
+// the targets' sums (as far_pair), the lane sums Gamma_i K (dz_ij, dx_ij) over
+// its targets i for this source j; the source's own sums receive them with the
+// opposite sign (dx_ji = -dx_ij).  Padding targets carry Gamma 0.
+__device__ __forceinline__ void mutual_pair(uint64_t sx, uint64_t sz, uint64_t sg,
+                                            const uint64_t (&tx2)[kWP],
+                                            const uint64_t (&tz2)[kWP],
+                                            const uint64_t (&tg2)[kWP], uint64_t (&nu2)[kWP],
+                                            uint64_t (&w2)[kWP], uint64_t& snu, uint64_t& sw) {
+#pragma unroll
+    for (int q = 0; q < kWP; ++q) {
+        const uint64_t dx = f2sub(tx2[q], sx);
+        const uint64_t dz = f2sub(tz2[q], sz);
+        const uint64_t r2 = f2fma(dx, dx, f2mul(dz, dz));
+        const uint64_t inv = f2pack(rcp_approx(f2lo(r2)), rcp_approx(f2hi(r2)));
+        const uint64_t g = f2mul(inv, sg);
+        nu2[q] = f2fma(g, dz, nu2[q]);
+        w2[q] = f2fma(g, dx, w2[q]);
+        const uint64_t h = f2mul(inv, tg2[q]);
+        snu = q ? f2fma(h, dz, snu) : f2mul(h, dz);
+        sw = q ? f2fma(h, dx, sw) : f2mul(h, dx);
+    }
+}
+
+// Sum of v[0..8) over the warp's 32 lanes by recursive halving: at distance
+// 16, 8, 4 each lane keeps half of its values and adds its partner's copy of
+// them, then two butterflies finish.  Lane l returns the total of value
+// (l >> 2) & 7 (a fixed tree, so the bits do not depend on timing).
+__device__ __forceinline__ float warp_sum8(float (&v)[8], int lane) {
+    const unsigned all = 0xffffffffu;
+    const bool u16 = lane & 16, u8 = lane & 8, u4 = lane & 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float send = u16 ? v[k] : v[k + 4];
+        v[k] = (u16 ? v[k + 4] : v[k]) + __shfl_xor_sync(all, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const float send = u8 ? v[k] : v[k + 2];
+        v[k] = (u8 ? v[k + 2] : v[k]) + __shfl_xor_sync(all, send, 8);
+    }
+    const float send = u4 ? v[0] : v[1];
+    float r = (u4 ? v[1] : v[0]) + __shfl_xor_sync(all, send, 4);
+    r += __shfl_xor_sync(all, r, 2);
+    r += __shfl_xor_sync(all, r, 1);
+    return r;
+}
+
+// A mutual far stage: sources in batches of four; per batch the eight
+// warp-wide sums (Gamma_i K dz and Gamma_i K dx for each source) go to the
+// sources' 64-bit fixed-point accumulators acc[2 j], acc[2 j + 1] (value x
+// 2^shift, rounded; integer addition is exact and order-free, so the sums do
+// not depend on which warp adds first).  Sources j >= n are padding.
+__device__ __forceinline__ void stage_mutual(const StagedTile& __restrict__ src,
+                                             const uint64_t (&tx2)[kWP],
+                                             const uint64_t (&tz2)[kWP],
+                                             const uint64_t (&tg2)[kWP], uint64_t (&nu2)[kWP],
+                                             uint64_t (&w2)[kWP],
+                                             unsigned long long* __restrict__ acc,
+                                             uint32_t nsrc, double scale, int lane) {
+    const int vi = (lane >> 2) & 7;  // the sum this lane ends with
+#pragma unroll 1
+    for (int i = 0; i < kBsST / 2; i += 2) {
+        const float4 P0 = src.pos2[i], P1 = src.pos2[i + 1];
+        const float4 G0 = src.gam2[i], G1 = src.gam2[i + 1];
+        uint64_t snu[4], sw[4];
+        mutual_pair(f2pack(P0.x, P0.x), f2pack(P0.y, P0.y), f2pack(G0.x, G0.y), tx2, tz2, tg2,
+                    nu2, w2, snu[0], sw[0]);
+        mutual_pair(f2pack(P0.z, P0.z), f2pack(P0.w, P0.w), f2pack(G0.z, G0.w), tx2, tz2, tg2,
+                    nu2, w2, snu[1], sw[1]);
+        mutual_pair(f2pack(P1.x, P1.x), f2pack(P1.y, P1.y), f2pack(G1.x, G1.y), tx2, tz2, tg2,
+                    nu2, w2, snu[2], sw[2]);
+        mutual_pair(f2pack(P1.z, P1.z), f2pack(P1.w, P1.w), f2pack(G1.z, G1.w), tx2, tz2, tg2,
+                    nu2, w2, snu[3], sw[3]);
+        float v[8];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            v[b] = f2lo(snu[b]) + f2hi(snu[b]);
+            v[4 + b] = f2lo(sw[b]) + f2hi(sw[b]);
+        }
+        const float r = warp_sum8(v, lane);
+        const uint32_t j = 2 * i + (vi & 3);
+        if ((lane & 3) == 0 && j < nsrc)
+            atomicAdd(&acc[2 * j + (vi >> 2)], (unsigned long long)__double2ll_rn((double)r * scale));
     }
 }
 
@@ -324,15 +436,28 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     s = t;
 }
 
-template <int WR, int MINB>
+// Scale exponent of a simulation's mutual fixed-point sums.  Each sum is below
+// n max|Gamma| / r_min with r_min^2 > min 10 sigma^2 (or 1e-30) over the mutual
+// far pairs, and k_pack bounds max|Gamma| < 2^mexp[0], 1/sqrt(min) <= 2^mexp[1];
+// so |sum| 2^shift < 2^58, well inside 64 bits, with a resolution of 2^-58 of
+// that bound (below 1e-17 of it; the FP32 terms carry 6e-8).
+__device__ __forceinline__ int mutual_shift(const int* __restrict__ mexp, int inst, uint32_t n) {
+    const int lgn = n > 1 ? 32 - __clz(n - 1) : 0;
+    const long long e = (long long)lgn + mexp[2 * inst] + mexp[2 * inst + 1];
+    return (int)max(-1000ll, min(1000ll, 58 - e));
+}
+
+template <int MINB>
 __global__ void __launch_bounds__(32 * kWWarps, MINB)
     k_self_f32(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
                const double2* __restrict__ pxz, const float4* __restrict__ pf,
                const TileMeta* __restrict__ meta, double2* __restrict__ part,
+               unsigned long long* __restrict__ macc, const int* __restrict__ mexp,
                unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ StagedTile s_src[kWWarps];
-    constexpr int kWP = WR / 2, kWTT = 32 * WR;
+    constexpr int kWTT = 32 * kWR;
+    static_assert(kWTT == kBsST, "a work item's targets are one sort tile");
     if (threadIdx.x == 0) {
         unsigned acc = 0;
         for (int k = 0; k < nlist; ++k) {
@@ -362,38 +487,45 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
         const uint32_t j0 = c * cs, j1 = min(n, j0 + cs);
         const double2* __restrict__ X = pxz + e.coff;
         const float4* __restrict__ F = pf + e.coff;
-        // FP32 offsets are taken from the first target of the enclosing
-        // 256-target block, whatever the item size, so every item shape rounds
-        // a pair's offsets identically
-        const double2 o = X[t0 - t0 % 256u];
+        // FP32 offsets from the tile's first target
+        const double2 o = X[t0];
+        const double scale = ldexp(1.0, mutual_shift(mexp, e.inst, n));
 
-        uint64_t tx2[kWP], tz2[kWP];
-        const uint32_t tb = t0 + lane * WR;
+        uint64_t tx2[kWP], tz2[kWP], tg2[kWP];
+        const uint32_t tb = t0 + lane * kWR;
 #pragma unroll
         for (int q = 0; q < kWP; ++q) {
-            float xs[2], zs[2];
+            float xs[2], zs[2], gs[2];
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
-                xs[h] = 0.0f;  // padding targets sit on the origin (a real target)
+                xs[h] = 0.0f;  // padding targets sit on the origin (a real target), Gamma 0
                 zs[h] = 0.0f;
+                gs[h] = 0.0f;
                 const uint32_t t = tb + 2 * q + h;
                 if (t < n) {
                     const double2 p = X[t];
                     xs[h] = (float)(p.x - o.x);
                     zs[h] = (float)(p.y - o.y);
+                    gs[h] = F[t].x;
                 }
             }
             tx2[q] = f2pack(xs[0], xs[1]);
             tz2[q] = f2pack(zs[0], zs[1]);
+            tg2[q] = f2pack(gs[0], gs[1]);
         }
-        // The near/far test uses the box of the enclosing 256-target block
-        // (its sort tile), the same for every item shape.
         const TileMeta& tm = meta[(e.coff + t0) / kBsST];
-        float su[WR], cu[WR], sw[WR], cw[WR];  // Kahan sums of -u and w
+        float su[kWR], cu[kWR], sw[kWR], cw[kWR];  // Kahan sums of -u and w
 #pragma unroll
-        for (int r = 0; r < WR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
+        for (int r = 0; r < kWR; ++r) su[r] = cu[r] = sw[r] = cw[r] = 0.0f;
 
         for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
+            const TileMeta m = meta[(e.coff + s0) / kBsST];
+            const double gx = fmax(0.0, fmax(m.xmin - tm.xmax, tm.xmin - m.xmax));
+            const double gz = fmax(0.0, fmax(m.zmin - tm.zmax, tm.zmin - m.zmax));
+            const double g2 = gx * gx + gz * gz;
+            // the same test in both tiles' items (symmetric in the two tiles)
+            const bool mutual = g2 > fmax(m.thr, tm.thr) * 1.001 + 1e-30;
+            if (mutual && s0 < t0) continue;  // the source tile's item adds this stage
             __syncwarp();
 #pragma unroll
             for (int q = 0; q < kBsST / 32; ++q) {
@@ -411,13 +543,13 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
                 }
             }
             __syncwarp();
-            const TileMeta m = meta[(e.coff + s0) / kBsST];
-            const double gx = fmax(0.0, fmax(m.xmin - tm.xmax, tm.xmin - m.xmax));
-            const double gz = fmax(0.0, fmax(m.zmin - tm.zmax, tm.zmin - m.zmax));
             uint64_t nu2[kWP], w2[kWP];
 #pragma unroll
             for (int q = 0; q < kWP; ++q) nu2[q] = w2[q] = 0ull;  // +0.0f in both halves
-            if (gx * gx + gz * gz > m.thr * 1.001 + 1e-30) {
+            if (mutual) {
+                stage_mutual(wsrc, tx2, tz2, tg2, nu2, w2, macc + 2 * (e.coff + s0),
+                             min((uint32_t)kBsST, j1 - s0), scale, lane);
+            } else if (g2 > m.thr * 1.001 + 1e-30) {
                 stage_far(wsrc, tx2, tz2, nu2, w2);
             } else {
                 stage_near(wsrc, tx2, tz2, nu2, w2);
@@ -432,7 +564,7 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
         }
         double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
 #pragma unroll
-        for (int r = 0; r < WR; ++r)
+        for (int r = 0; r < kWR; ++r)
             if (tb + r < n)
                 out[tb + r] = make_double2(-((double)su[r] - (double)cu[r]),
                                            (double)sw[r] - (double)cw[r]);
@@ -516,7 +648,9 @@ __global__ void k_self_combine(const InstDesc* __restrict__ table,
                                const InstState* __restrict__ st,
                                const ListEntry* __restrict__ list, int nlist,
                                const uint32_t* __restrict__ perm,
-                               const double2* __restrict__ part) {
+                               const double2* __restrict__ part,
+                               const unsigned long long* __restrict__ macc,
+                               const int* __restrict__ mexp) {
     __shared__ unsigned s_pre[kMaxList + 1];
     if (threadIdx.x == 0) {
         unsigned acc = 0;
@@ -539,6 +673,12 @@ __global__ void k_self_combine(const InstDesc* __restrict__ table,
             const double2 v = part[e.poff + (uint64_t)c * e.cap + t];
             su += v.x;
             sw += v.y;
+        }
+        if (macc) {  // what the mutual far tiles gave this blob as a source
+            const double inv = ldexp(1.0, -mutual_shift(mexp, e.inst, n));
+            const uint64_t g = 2 * (e.coff + t);
+            su += (double)(long long)macc[g] * inv;
+            sw -= (double)(long long)macc[g + 1] * inv;
         }
         const InstDesc& d = table[e.inst];
         const uint32_t p = perm ? perm[e.coff + t] : t;
@@ -886,7 +1026,10 @@ void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* 
     double2* pxz = precision == kF32 ? reinterpret_cast<double2*>(ws.packed) : nullptr;
     float4* pf = precision == kF32 ? reinterpret_cast<float4*>(ws.packed + ws.packed_cap / 2)
                                    : nullptr;
-    k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, pxz, pf, ws.meta);
+    if (precision == kF32)  // 0x80808080 per exponent: below any bound k_pack writes
+        cudaMemsetAsync(ws.mexp, 0x80, sizeof(int) * 2 * kTableCap, s);
+    k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, pxz, pf, ws.meta,
+                                     precision == kF32 ? ws.mexp : nullptr);
     cudaMemsetAsync(ws.work, 0, sizeof(unsigned), s);
 }
 
@@ -897,13 +1040,10 @@ void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* 
     if (precision == kF32) {
         const double2* pxz = reinterpret_cast<const double2*>(ws.packed);
         const float4* pf = reinterpret_cast<const float4*>(ws.packed + ws.packed_cap / 2);
-        const int g = sms * std::max(1, std::min(cfg.ctas, 4));
-        if (cfg.tile == 128)
-            k_self_f32<4, 4><<<g, 32 * kWWarps, 0, s>>>(st, list, nlist, pxz, pf, ws.meta,
-                                                         ws.part, ws.work);
-        else
-            k_self_f32<8, kSelfMinBlocks><<<g, 32 * kWWarps, 0, s>>>(
-                st, list, nlist, pxz, pf, ws.meta, ws.part, ws.work);
+        const int g = sms * std::max(1, std::min(cfg.ctas, kSelfMinBlocks));
+        cudaMemsetAsync(ws.macc, 0, 16 * ws.total_cap, s);
+        k_self_f32<kSelfMinBlocks><<<g, 32 * kWWarps, 0, s>>>(
+            st, list, nlist, pxz, pf, ws.meta, ws.part, ws.macc, ws.mexp, ws.work);
     } else {
         k_self_f64<<<sms * kF64Ctas, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part,
                                                              ws.work);
@@ -912,8 +1052,9 @@ void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* 
 
 void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                         int precision, const Workspace& ws, int sms, cudaStream_t s) {
-    k_self_combine<<<sms * 8, 256, 0, s>>>(table, st, list, nlist,
-                                           precision == kF32 ? ws.perm : nullptr, ws.part);
+    const bool f32 = precision == kF32;
+    k_self_combine<<<sms * 8, 256, 0, s>>>(table, st, list, nlist, f32 ? ws.perm : nullptr,
+                                           ws.part, f32 ? ws.macc : nullptr, ws.mexp);
 }
 
 void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,

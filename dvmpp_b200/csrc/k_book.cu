@@ -22,23 +22,63 @@ __device__ __forceinline__ void raise_status(InstState& s, int code) {
 }
 
 // ---- diffusion -------------------------------------------------------------------
+// One flat index space over the blobs of every simulation in the list, so the
+// grid's threads get equal shares whatever the sizes (a simulation of 4e5 blobs
+// beside ones of 1e4).  A failed simulation, or one whose injected stream cannot
+// cover this step, contributes no blobs; block 0 flags the exhausted stream.
+__device__ __forceinline__ int locate64(const uint64_t* pre, int nlist, uint64_t g) {
+    int lo = 0, hi = nlist - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 __global__ void k_diffuse(const InstDesc* __restrict__ table, InstState* __restrict__ st,
                           const ListEntry* __restrict__ list, int nlist) {
-    const ListEntry e = list[blockIdx.y];
-    const InstDesc& d = table[e.inst];
-    InstState& S = st[e.inst];
-    if (S.status) return;
-    const uint32_t n = S.n;
-    const uint64_t cur = S.cursor;
-    if (d.rng == kInject && cur + 2ull * n > d.ucount) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(S, kErrRngExhausted);
-        return;
+    __shared__ uint64_t s_pre[kMaxBatch + 1];
+    const int tid = threadIdx.x;
+    for (int k = tid; k < nlist; k += blockDim.x) {
+        const int inst = list[k].inst;
+        InstState& S = st[inst];
+        uint32_t n = S.status ? 0u : S.n;
+        if (n && table[inst].rng == kInject && S.cursor + 2ull * n > table[inst].ucount) {
+            if (blockIdx.x == 0) raise_status(S, kErrRngExhausted);
+            n = 0;
+        }
+        s_pre[k + 1] = n;
     }
-    const double c4 = dmul(dmul(4.0, d.nu), d.dt);
+    __syncthreads();
+    if (tid < 32) {  // inclusive scan of the counts, 32 simulations per pass
+        uint64_t carry = 0;
+        for (int b = 0; b < nlist; b += 32) {
+            const int k = b + tid;
+            uint64_t v = k < nlist ? s_pre[k + 1] : 0ull;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint64_t t = __shfl_up_sync(0xffffffffu, v, o);
+                if (tid >= o) v += t;
+            }
+            if (k < nlist) s_pre[k + 1] = v + carry;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (tid == 0) s_pre[0] = 0;
+    }
+    __syncthreads();
+    const uint64_t total = s_pre[nlist];
     const double twopi = dmul(2.0, kPi);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + tid; g < total;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = locate64(s_pre, nlist, g);
+        const uint32_t i = (uint32_t)(g - s_pre[k]);
+        const int inst = list[k].inst;
+        const InstDesc& d = table[inst];
+        const InstState& S = st[inst];
+        const double c4 = dmul(dmul(4.0, d.nu), d.dt);
         double R1, R2;
         if (d.rng == kInject) {
+            const uint64_t cur = S.cursor;
             R1 = d.uniforms[cur + 2ull * i];
             R2 = d.uniforms[cur + 2ull * i + 1];
         } else {
@@ -534,8 +574,7 @@ void diffuse(const InstDesc* table, InstState* st, const ListEntry* list, int nl
              const Workspace& ws, int sms, cudaStream_t s) {
     (void)ws;
     // many resident warps: each blob is a chain of FP64 log / sqrt / sincos
-    dim3 g(std::max(1, sms * 32 / std::max(1, nlist)), nlist);
-    k_diffuse<<<g, 256, 0, s>>>(table, st, list, nlist);
+    k_diffuse<<<sms * 16, 256, 0, s>>>(table, st, list, nlist);
 }
 
 void diffuse_raw(double* x, double* z, uint32_t n, const double* R, double nu, double dt,

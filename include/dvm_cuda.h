@@ -373,16 +373,17 @@ int dvm_batch_wait_state(dvm_ctx* ctx, int nsims, double* const* x, double* cons
                          double* loads);
 
 /* ---- pair-kernel autotuning (no counterpart in the reference) ---------------------
- * The FP32 blob-on-blob kernel's launch shape: targets per work item, persistent
- * CTAs per SM and the order in which simulations' work items are handed out.
- * None of these changes a result (source chunking, which would, is fixed by each
- * simulation's capacity), so tuning never changes velocities.  Shapes are kept
+ * The FP32 blob-on-blob kernel's launch shape: persistent CTAs per SM and the
+ * order in which simulations' work items are handed out (a work item is one
+ * 256-blob sort tile of targets against one source chunk).  Neither changes a
+ * result (source chunking, which would, is fixed by each simulation's capacity),
+ * so tuning never changes velocities.  Shapes are kept
  * per batch-shape class (log2 of the summed capacity of the batch's FP32
  * simulations x a bucket of their count: 1, 2-8, 9-64, more); plans and graphs
  * built afterwards use them. */
 typedef struct dvm_pair_config {
-    int32_t tile;        /* targets per work item: 256 or 128 */
-    int32_t ctas_per_sm; /* 1..3 for 256-target items, 1..4 for 128 */
+    int32_t tile;        /* targets per work item: 256 */
+    int32_t ctas_per_sm; /* 1..3 */
     int32_t order;       /* 0: list order; 1: costliest simulations' items first */
     int32_t reserved;
 } dvm_pair_config;
@@ -400,7 +401,7 @@ typedef struct dvm_tune_result {
 /* The search space, enumerated: index 0 .. count-1; DVM_ERR_ARG past the end. */
 int dvm_tune_candidate(int index, dvm_pair_config* out);
 /* Time every candidate on this batch's FP32 simulations (reps launches each,
- * after one untimed launch per kernel variant) and store the fastest for the
+ * after one untimed launch) and store the fastest for the
  * batch's class.  Simulation state is not modified (the pair kernel writes only
  * workspace partials; the next step recomputes velocities).  Synchronous: meant
  * for set-up (or once per class in a long-running server), not per step. */

@@ -1,7 +1,9 @@
 """The pair-kernel autotuner: every launch shape in its search space gives
-bitwise-identical steps (targets per item, CTAs per SM and item order never
-change a target's operation sequence; source chunking, which would, is fixed by
-capacity), and autotune() keeps the fastest shape for the batch's class."""
+bitwise-identical steps (CTAs per SM and item order never change a target's
+operation sequence, and the mutual far tiles' fixed-point sums do not depend on
+the order their terms arrive in; source chunking, which would change results,
+is fixed by capacity), and autotune() keeps the fastest shape for the batch's
+class; shapes outside the search space are refused."""
 import numpy as np
 import pytest
 
@@ -69,10 +71,10 @@ def test_autotune_keeps_the_fastest_for_the_class(ctx):
 
 
 def test_tuning_table_round_trip(ctx, tmp_path):
-    ctx.set_pair_config(7, 128, 2, 1)
+    ctx.set_pair_config(7, 256, 2, 1)
     ctx.set_pair_config(41, 256, 1, 0)
     table = ctx.tuning_table()
-    assert table[7] == {"tile": 128, "ctas_per_sm": 2, "order": 1}
+    assert table[7] == {"tile": 256, "ctas_per_sm": 2, "order": 1}
     assert table[41] == {"tile": 256, "ctas_per_sm": 1, "order": 0}
     path = tmp_path / "tuning.json"
     ctx.save_tuning(str(path))
@@ -81,6 +83,8 @@ def test_tuning_table_round_trip(ctx, tmp_path):
     assert other.tuning_table() == table
     other.close()
     with pytest.raises(N.DvmError):
-        ctx.set_pair_config(3, 256, 4, 0)  # 256-target items allow 1..3 CTAs per SM
+        ctx.set_pair_config(3, 256, 4, 0)  # 1..3 CTAs per SM
+    with pytest.raises(N.DvmError):
+        ctx.set_pair_config(3, 128, 2, 0)  # work items are one 256-blob tile
     ctx.set_pair_config(-1, 256, 3, 0)
     assert ctx.tuning_table() == {}
