@@ -104,7 +104,7 @@ std::vector<ListEntry> costliest_first(const std::vector<ListEntry>& h) {
 
 bool valid_pair_config(const dvm_pair_config& p) {
     if (p.tile != 256) return false;
-    if (p.ctas_per_sm < 1 || p.ctas_per_sm > 3) return false;
+    if (p.ctas_per_sm < 1 || p.ctas_per_sm > 4) return false;
     return p.order == 0 || p.order == 1;
 }
 
@@ -1936,8 +1936,8 @@ int dvm_step_batch(dvm_ctx* c, dvm_sim* const* sims, int nsims, int nsteps, int 
 // ---- pair-kernel autotuning ------------------------------------------------------------
 namespace {
 const dvm_pair_config kCandidates[] = {
-    {256, 3, 0, 0}, {256, 2, 0, 0}, {256, 1, 0, 0}, {256, 3, 1, 0}, {256, 2, 1, 0},
-    {256, 1, 1, 0}};
+    {256, 4, 0, 0}, {256, 3, 0, 0}, {256, 2, 0, 0}, {256, 4, 1, 0}, {256, 3, 1, 0},
+    {256, 2, 1, 0}};
 constexpr int kNumCandidates = (int)(sizeof(kCandidates) / sizeof(kCandidates[0]));
 static_assert(kNumCandidates <= DVM_TUNE_MAX_CANDIDATES, "candidate table too long");
 

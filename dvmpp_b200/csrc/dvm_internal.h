@@ -183,8 +183,8 @@ size_t cub_sort_bytes(uint64_t total);
 // Launch shape of the FP32 pair kernel.  None of it changes a result: the
 // source chunking (which does) is fixed by each simulation's capacity.
 struct PairConfig {
-    int tile = 256;  // targets per work item: 256 or 128
-    int ctas = 3;    // persistent CTAs per SM
+    int tile = 256;  // targets per work item (one sort tile)
+    int ctas = 4;    // persistent CTAs per SM
     int order = 0;   // 0: list order; 1: costliest simulations' items first (the caller
                      // passes the list in that order)
 };

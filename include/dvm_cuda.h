@@ -383,7 +383,7 @@ int dvm_batch_wait_state(dvm_ctx* ctx, int nsims, double* const* x, double* cons
  * built afterwards use them. */
 typedef struct dvm_pair_config {
     int32_t tile;        /* targets per work item: 256 */
-    int32_t ctas_per_sm; /* 1..3 */
+    int32_t ctas_per_sm; /* 1..4 */
     int32_t order;       /* 0: list order; 1: costliest simulations' items first */
     int32_t reserved;
 } dvm_pair_config;
@@ -394,7 +394,7 @@ typedef struct dvm_tune_result {
     int32_t shape_class;
     int32_t candidates;          /* configurations timed (dvm_tune_candidate order) */
     double best_ms;              /* mean pair-kernel time of the best */
-    double default_ms;           /* mean time of the built-in shape (256, 3, 0) */
+    double default_ms;           /* mean time of the built-in shape (256, 4, 0) */
     double ms[DVM_TUNE_MAX_CANDIDATES];
 } dvm_tune_result;
 

@@ -48,7 +48,7 @@ def test_every_shape_gives_identical_steps(ctx):
         for a, b in zip(got, ref):
             for key in ("x", "z", "u", "w", "uvs", "wvs"):
                 assert np.array_equal(a[key], b[key]), (cand, key)
-    ctx.set_pair_config(-1, 256, 3, 0)
+    ctx.set_pair_config(-1, 256, 4, 0)
 
 
 def test_autotune_keeps_the_fastest_for_the_class(ctx):
@@ -64,7 +64,7 @@ def test_autotune_keeps_the_fastest_for_the_class(ctx):
     for s in sims:
         s.check()
         s.close()
-    ctx.set_pair_config(-1, 256, 3, 0)  # back to the default shape, table cleared
+    ctx.set_pair_config(-1, 256, 4, 0)  # back to the default shape, table cleared
     ref = _run(ctx)
     for a, b in zip(tuned, ref):
         assert np.array_equal(a["u"], b["u"]) and np.array_equal(a["x"], b["x"])
@@ -83,8 +83,8 @@ def test_tuning_table_round_trip(ctx, tmp_path):
     assert other.tuning_table() == table
     other.close()
     with pytest.raises(N.DvmError):
-        ctx.set_pair_config(3, 256, 4, 0)  # 1..3 CTAs per SM
+        ctx.set_pair_config(3, 256, 5, 0)  # 1..4 CTAs per SM
     with pytest.raises(N.DvmError):
         ctx.set_pair_config(3, 128, 2, 0)  # work items are one 256-blob tile
-    ctx.set_pair_config(-1, 256, 3, 0)
+    ctx.set_pair_config(-1, 256, 4, 0)
     assert ctx.tuning_table() == {}
