@@ -268,9 +268,9 @@ __device__ __forceinline__ void stage_far(const StagedTile& __restrict__ src,
 }
 
 // Mutual far pairs: one reciprocal per pair serves both directions.  Besides
-// the targets' sums (as far_pair), the lane sums Gamma_i K (dz_ij, dx_ij) over
-// its targets i for this source j; the source's own sums receive them with the
-// opposite sign (dx_ji = -dx_ij).  Padding targets carry Gamma 0.
+// the targets' sums (as far_pair), the lane adds Gamma_i K (dz_ij, dx_ij) of its
+// targets i to source j's packed sums snu, sw; the source's own velocity takes
+// them with the opposite sign (dx_ji = -dx_ij).  Padding targets carry Gamma 0.
 __device__ __forceinline__ void mutual_pair(uint64_t sx, uint64_t sz, uint64_t sg,
                                             const uint64_t (&tx2)[kWP],
                                             const uint64_t (&tz2)[kWP],
@@ -286,40 +286,22 @@ __device__ __forceinline__ void mutual_pair(uint64_t sx, uint64_t sz, uint64_t s
         nu2[q] = f2fma(g, dz, nu2[q]);
         w2[q] = f2fma(g, dx, w2[q]);
         const uint64_t h = f2mul(inv, tg2[q]);
-        snu = q ? f2fma(h, dz, snu) : f2mul(h, dz);
-        sw = q ? f2fma(h, dx, sw) : f2mul(h, dx);
+        snu = f2fma(h, dz, snu);
+        sw = f2fma(h, dx, sw);
     }
 }
 
-// Sum of v[0..8) over the warp's 32 lanes by recursive halving: at distance
-// 16, 8, 4 each lane keeps half of its values and adds its partner's copy of
-// them, then two butterflies finish.  Lane l returns the total of value
-// (l >> 2) & 7 (a fixed tree, so the bits do not depend on timing).
-__device__ __forceinline__ float warp_sum8(float (&v)[8], int lane) {
-    const unsigned all = 0xffffffffu;
-    const bool u16 = lane & 16, u8 = lane & 8, u4 = lane & 4;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float send = u16 ? v[k] : v[k + 4];
-        v[k] = (u16 ? v[k + 4] : v[k]) + __shfl_xor_sync(all, send, 16);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const float send = u8 ? v[k] : v[k + 2];
-        v[k] = (u8 ? v[k + 2] : v[k]) + __shfl_xor_sync(all, send, 8);
-    }
-    const float send = u4 ? v[0] : v[1];
-    float r = (u4 ? v[1] : v[0]) + __shfl_xor_sync(all, send, 4);
-    r += __shfl_xor_sync(all, r, 2);
-    r += __shfl_xor_sync(all, r, 1);
-    return r;
-}
-
-// A mutual far stage: sources in batches of four; per batch the eight
-// warp-wide sums (Gamma_i K dz and Gamma_i K dx for each source) go to the
-// sources' 64-bit fixed-point accumulators acc[2 j], acc[2 j + 1] (value x
-// 2^shift, rounded; integer addition is exact and order-free, so the sums do
-// not depend on which warp adds first).  Sources j >= n are padding.
+// A mutual far stage.  The staged sources form 64 groups of four, taken in
+// two rounds of 32.  In step s of a round lane l evaluates group (l + s) mod 32
+// against its 8 targets, adding to the group's packed sums (Gamma_i K dz,
+// Gamma_i K dx per source; low and high halves from the even and odd targets),
+// then hands the sums to lane l - 1, which takes that group in step s + 1.
+// After 32 steps lane l holds the sums of group l over all 256 targets, in a
+// fixed order, and adds them to the sources' 64-bit fixed-point accumulators
+// acc[2 j], acc[2 j + 1] (value x 2^shift, rounded; integer addition is exact
+// and order-free, so the sums do not depend on which warp adds first).  The
+// hand-over costs 16 shuffles per 32 pairs and no arithmetic (a shuffle-tree
+// reduction per batch of sources was 3.5 % slower).  Sources j >= n are padding.
 __device__ __forceinline__ void stage_mutual(const StagedTile& __restrict__ src,
                                              const uint64_t (&tx2)[kWP],
                                              const uint64_t (&tz2)[kWP],
@@ -327,30 +309,44 @@ __device__ __forceinline__ void stage_mutual(const StagedTile& __restrict__ src,
                                              uint64_t (&w2)[kWP],
                                              unsigned long long* __restrict__ acc,
                                              uint32_t nsrc, double scale, int lane) {
-    const int vi = (lane >> 2) & 7;  // the sum this lane ends with
+    const unsigned all = 0xffffffffu;
+    const int next = (lane + 1) & 31;
 #pragma unroll 1
-    for (int i = 0; i < kBsST / 2; i += 2) {
-        const float4 P0 = src.pos2[i], P1 = src.pos2[i + 1];
-        const float4 G0 = src.gam2[i], G1 = src.gam2[i + 1];
-        uint64_t snu[4], sw[4];
-        mutual_pair(f2pack(P0.x, P0.x), f2pack(P0.y, P0.y), f2pack(G0.x, G0.y), tx2, tz2, tg2,
-                    nu2, w2, snu[0], sw[0]);
-        mutual_pair(f2pack(P0.z, P0.z), f2pack(P0.w, P0.w), f2pack(G0.z, G0.w), tx2, tz2, tg2,
-                    nu2, w2, snu[1], sw[1]);
-        mutual_pair(f2pack(P1.x, P1.x), f2pack(P1.y, P1.y), f2pack(G1.x, G1.y), tx2, tz2, tg2,
-                    nu2, w2, snu[2], sw[2]);
-        mutual_pair(f2pack(P1.z, P1.z), f2pack(P1.w, P1.w), f2pack(G1.z, G1.w), tx2, tz2, tg2,
-                    nu2, w2, snu[3], sw[3]);
-        float v[8];
+    for (int rnd = 0; rnd < kBsST / 128; ++rnd) {
+        uint64_t au[4], aw[4];  // packed sums of the group this lane holds
+#pragma unroll
+        for (int b = 0; b < 4; ++b) au[b] = aw[b] = 0ull;
+#pragma unroll 1
+        for (int s = 0; s < 32; ++s) {
+            const int gi = rnd * 32 + ((lane + s) & 31);  // group of 4 sources
+            const float4 P0 = src.pos2[2 * gi], P1 = src.pos2[2 * gi + 1];
+            const float4 G0 = src.gam2[2 * gi], G1 = src.gam2[2 * gi + 1];
+            mutual_pair(f2pack(P0.x, P0.x), f2pack(P0.y, P0.y), f2pack(G0.x, G0.y), tx2, tz2,
+                        tg2, nu2, w2, au[0], aw[0]);
+            mutual_pair(f2pack(P0.z, P0.z), f2pack(P0.w, P0.w), f2pack(G0.z, G0.w), tx2, tz2,
+                        tg2, nu2, w2, au[1], aw[1]);
+            mutual_pair(f2pack(P1.x, P1.x), f2pack(P1.y, P1.y), f2pack(G1.x, G1.y), tx2, tz2,
+                        tg2, nu2, w2, au[2], aw[2]);
+            mutual_pair(f2pack(P1.z, P1.z), f2pack(P1.w, P1.w), f2pack(G1.z, G1.w), tx2, tz2,
+                        tg2, nu2, w2, au[3], aw[3]);
+            // the group moves on to the lane that takes it next (lane - 1)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                au[b] = __shfl_sync(all, au[b], next);
+                aw[b] = __shfl_sync(all, aw[b], next);
+            }
+        }
+        // after 32 steps every lane's targets have passed over the group this lane holds
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            v[b] = f2lo(snu[b]) + f2hi(snu[b]);
-            v[4 + b] = f2lo(sw[b]) + f2hi(sw[b]);
+            const uint32_t j = 4 * (rnd * 32 + lane) + b;
+            if (j < nsrc) {
+                atomicAdd(&acc[2 * j], (unsigned long long)__double2ll_rn(
+                                           (double)(f2lo(au[b]) + f2hi(au[b])) * scale));
+                atomicAdd(&acc[2 * j + 1], (unsigned long long)__double2ll_rn(
+                                               (double)(f2lo(aw[b]) + f2hi(aw[b])) * scale));
+            }
         }
-        const float r = warp_sum8(v, lane);
-        const uint32_t j = 2 * i + (vi & 3);
-        if ((lane & 3) == 0 && j < nsrc)
-            atomicAdd(&acc[2 * j + (vi >> 2)], (unsigned long long)__double2ll_rn((double)r * scale));
     }
 }
 
