@@ -56,13 +56,14 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 // Source chunks of a simulation's pair kernel.  Fixed by the capacity alone, so
 // a simulation's sums are associated the same way alone and inside any batch:
-// at least one chunk per 64 k sources, and for small simulations enough chunks
-// (>= ~2^21 / cap items per 256-target tile) to occupy the GPU when stepped
-// alone, but never chunks shorter than 8 k sources.
+// at least one chunk per 32 k sources (up to 32), and for small simulations
+// enough chunks (~2^23 / cap per 256-target tile, ~32 k work items) to occupy
+// the GPU when stepped alone, but never chunks shorter than 512 sources.  In
+// FP32 a chunk costs two 64-bit atomic adds per target (FP64: a partial sum).
 int nbody_chunks(uint32_t cap) {
-    const int by_size = (int)std::min<uint32_t>(16, (cap + 65535) / 65536);
-    const int by_fill = (int)((2u << 20) / std::max<uint32_t>(cap, 1));
-    const int most = (int)std::max<uint32_t>(1, std::min<uint32_t>(64, cap / 8192));
+    const int by_size = (int)std::min<uint32_t>(32, (cap + 32767) / 32768);
+    const int by_fill = (int)((8u << 20) / std::max<uint32_t>(cap, 1));
+    const int most = (int)std::max<uint32_t>(1, std::min<uint32_t>(64, cap / 512));
     return std::max(1, std::min(most, std::max(by_size, by_fill)));
 }
 
@@ -282,7 +283,8 @@ int build_sublist(dvm_ctx* c, SubList& sl, Plan& pl, bool f32_pairs = false) {
         e.roff = roff;
         e.cofs = cofs;
         coff += e.cap;  // caps are multiples of kCapAlign
-        poff += (uint64_t)e.chunks * e.cap;
+        if (s->h.precision != kF32)  // the FP32 path sums in fixed point, without partials
+            poff += (uint64_t)e.chunks * e.cap;
         roff += (uint64_t)e.rhs_chunks * e.npad;
         cofs += (uint64_t)e.rhs_chunks;
         sl.max_np = std::max(sl.max_np, s->h.np);
@@ -471,7 +473,7 @@ void issue_step(dvm_ctx* c, Plan& pl) {
         p = prof_begin(c, DVM_PROF_SORT);
         biot_savart_finish(T, S, sl.d_list, sl.n, prec, ws, sms, s);
         prof_end(c, p);
-        L += (prec == kF32) ? 4 : 3;
+        L += 4;  // keys, pack, pair kernel, combine
         p = prof_begin(c, DVM_PROF_RHS);
         sheet_rhs(T, S, sl.d_list, sl.n, sl.max_np, prec, ws, sms, s);
         prof_end(c, p);
@@ -2147,7 +2149,8 @@ static int raw_self(dvm_ctx* c, const double* x, const double* z, const double* 
     e.rhs_chunks = 1;
     e.rhs_chunk = kAtChunk;
     e.npad = 256;
-    int rc = ensure_workspace(c, cap, (uint64_t)e.chunks * cap, 256, 1, 1, false);
+    const uint64_t part = precision == kF32 ? 1 : (uint64_t)e.chunks * cap;  // FP64 partials
+    int rc = ensure_workspace(c, cap, part, 256, 1, 1, false);
     if (rc) return rc;
     ListEntry* d_list = reinterpret_cast<ListEntry*>(c->ws.jobs);
     InstState st0;
@@ -2161,7 +2164,7 @@ static int raw_self(dvm_ctx* c, const double* x, const double* z, const double* 
     ws.total_cap = cap;
     biot_savart_self(c->d_table, c->d_state, d_list, 1, precision, ws, c->sms, c->stream,
                      tuned_config(c, shape_class(cap, 1)));
-    g_launches += precision == kF32 ? 4 : 3;
+    g_launches += 4;  // keys, pack, pair kernel, combine
     CK(cudaGetLastError());
     return DVM_OK;
 }

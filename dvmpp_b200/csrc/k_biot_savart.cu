@@ -291,6 +291,12 @@ __device__ __forceinline__ void mutual_pair(uint64_t sx, uint64_t sz, uint64_t s
     }
 }
 
+// v 2^shift rounded to a 64-bit integer (two's complement in the unsigned
+// accumulator; the conversion saturates outside the 64-bit range).
+__device__ __forceinline__ unsigned long long to_fixed(double v, double scale) {
+    return (unsigned long long)__double2ll_rn(v * scale);
+}
+
 // A mutual far stage.  The staged sources form 64 groups of four, taken in
 // two rounds of 32.  In step s of a round lane l evaluates group (l + s) mod 32
 // against its 8 targets, adding to the group's packed sums (Gamma_i K dz,
@@ -340,11 +346,9 @@ __device__ __forceinline__ void stage_mutual(const StagedTile& __restrict__ src,
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const uint32_t j = 4 * (rnd * 32 + lane) + b;
-            if (j < nsrc) {
-                atomicAdd(&acc[2 * j], (unsigned long long)__double2ll_rn(
-                                           (double)(f2lo(au[b]) + f2hi(au[b])) * scale));
-                atomicAdd(&acc[2 * j + 1], (unsigned long long)__double2ll_rn(
-                                               (double)(f2lo(aw[b]) + f2hi(aw[b])) * scale));
+            if (j < nsrc) {  // u_j += sum Gamma_i K dz_ij, w_j -= sum Gamma_i K dx_ij
+                atomicAdd(&acc[2 * j], to_fixed((double)(f2lo(au[b]) + f2hi(au[b])), scale));
+                atomicAdd(&acc[2 * j + 1], to_fixed(-(double)(f2lo(aw[b]) + f2hi(aw[b])), scale));
             }
         }
     }
@@ -432,24 +436,25 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     s = t;
 }
 
-// Scale exponent of a simulation's mutual fixed-point sums.  Each sum is below
-// n max|Gamma| / r_min with r_min^2 > min 10 sigma^2 (or 1e-30) over the mutual
-// far pairs, and k_pack bounds max|Gamma| < 2^mexp[0], 1/sqrt(min) <= 2^mexp[1];
-// so |sum| 2^shift < 2^58, well inside 64 bits, with a resolution of 2^-58 of
-// that bound (below 1e-17 of it; the FP32 terms carry 6e-8).
+// Scale exponent of a simulation's fixed-point velocity sums.  One pair adds at
+// most |Gamma_j| K r: 1/r <= 1/sqrt(10 sigma_j^2) outside the core and at most
+// 0.64/sigma_j = 2.02/sqrt(10 sigma_j^2) inside it, so every sum is below
+// 2.02 n max|Gamma| / sqrt(min 10 sigma^2) (1e-30 as the floor of the minimum);
+// k_pack bounds max|Gamma| < 2^mexp[0] and 1/sqrt(min) <= 2^mexp[1].  With the
+// shift below |sum| 2^shift < 2^58, well inside 64 bits, and one unit is 2^-56
+// of the bound (below 2e-17 of it; the FP32 terms carry 6e-8).
 __device__ __forceinline__ int mutual_shift(const int* __restrict__ mexp, int inst, uint32_t n) {
     const int lgn = n > 1 ? 32 - __clz(n - 1) : 0;
     const long long e = (long long)lgn + mexp[2 * inst] + mexp[2 * inst + 1];
-    return (int)max(-1000ll, min(1000ll, 58 - e));
+    return (int)max(-1000ll, min(1000ll, 56 - e));
 }
 
 template <int MINB>
 __global__ void __launch_bounds__(32 * kWWarps, MINB)
     k_self_f32(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
                const double2* __restrict__ pxz, const float4* __restrict__ pf,
-               const TileMeta* __restrict__ meta, double2* __restrict__ part,
-               unsigned long long* __restrict__ macc, const int* __restrict__ mexp,
-               unsigned* __restrict__ work) {
+               const TileMeta* __restrict__ meta, unsigned long long* __restrict__ macc,
+               const int* __restrict__ mexp, unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ StagedTile s_src[kWWarps];
     // Kahan sums of -u and w per lane, in shared memory rather than registers
@@ -563,26 +568,37 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
                 kahan(kh[2][2 * q + 1][lane], kh[3][2 * q + 1][lane], f2hi(w2[q]));
             }
         }
-        double2* __restrict__ out = part + e.poff + (uint64_t)c * e.cap;
+        // the item's sums join the targets' fixed-point sums (exact, order-free)
+        unsigned long long* __restrict__ ta = macc + 2 * (e.coff + tb);
 #pragma unroll
         for (int r = 0; r < kWR; ++r)
-            if (tb + r < n)
-                out[tb + r] = make_double2(-((double)kh[0][r][lane] - (double)kh[1][r][lane]),
-                                           (double)kh[2][r][lane] - (double)kh[3][r][lane]);
+            if (tb + r < n) {
+                atomicAdd(&ta[2 * r],
+                          to_fixed(-((double)kh[0][r][lane] - (double)kh[1][r][lane]), scale));
+                atomicAdd(&ta[2 * r + 1],
+                          to_fixed((double)kh[2][r][lane] - (double)kh[3][r][lane], scale));
+            }
     }
 }
 
-// ---- FP64, reference operation order ---------------------------------------
+// ---- FP64, the reference's per-pair arithmetic -------------------------------
+// Every pair is evaluated with the reference's operations (src/VelocityKernel.cpp:
+// 44-60: IEEE division and exp inside the core, 1/r2 outside), over the same
+// Morton-sorted tiles as the FP32 path.  A source stage whose tile box is beyond
+// 10 sigma^2 of the item's target box (the union of its sort tiles) holds no core
+// pair and no self pair, and runs the 1/r2 branch without the per-pair test; in
+// blob order nearly every warp met a core pair somewhere and ran both branches.
 // 3 CTAs of 8 warps per SM (80 registers): the FP64 division / exp chains need
 // the warps (1 CTA per SM ran 2.2x slower)
 constexpr int kF64Ctas = 3;
 __global__ void __launch_bounds__(kBsThreads, kF64Ctas)
     k_self_f64(const InstState* __restrict__ st, const ListEntry* __restrict__ list, int nlist,
-               const double4* __restrict__ packed, double2* __restrict__ part,
-               unsigned* __restrict__ work) {
+               const double4* __restrict__ packed, const TileMeta* __restrict__ meta,
+               double2* __restrict__ part, unsigned* __restrict__ work) {
     __shared__ unsigned s_pre[kMaxList + 1];
     __shared__ double4 s_src[kBsST];  // x, z, circ, threshold
     __shared__ double s_rs[kBsST];
+    __shared__ double s_box[4];  // the item's target box: xmin, xmax, zmin, zmax
     __shared__ unsigned s_item;
     item_prefix_f64(s_pre, st, list, nlist);
     const unsigned total = s_pre[nlist];
@@ -610,17 +626,52 @@ __global__ void __launch_bounds__(kBsThreads, kF64Ctas)
             tz[r] = p.y;
             uu[r] = ww[r] = 0.0;
         }
+        if (tid == 0) {  // the item's target box (read after the next barrier)
+            double b0 = DBL_MAX, b1 = -DBL_MAX, b2 = DBL_MAX, b3 = -DBL_MAX;
+            for (int q = 0; q < kBsTT / kBsST; ++q) {
+                const uint32_t t = tile * kBsTT + q * kBsST;
+                if (t < n) {
+                    const TileMeta& m = meta[(e.coff + t) / kBsST];
+                    b0 = fmin(b0, m.xmin);
+                    b1 = fmax(b1, m.xmax);
+                    b2 = fmin(b2, m.zmin);
+                    b3 = fmax(b3, m.zmax);
+                }
+            }
+            s_box[0] = b0;
+            s_box[1] = b1;
+            s_box[2] = b2;
+            s_box[3] = b3;
+        }
         for (uint32_t s0 = j0; s0 < j1; s0 += kBsST) {
             __syncthreads();
+            const TileMeta& m = meta[(e.coff + s0) / kBsST];
+            const double gx = fmax(0.0, fmax(m.xmin - s_box[1], s_box[0] - m.xmax));
+            const double gz = fmax(0.0, fmax(m.zmin - s_box[3], s_box[2] - m.zmax));
+            const bool far = gx * gx + gz * gz > m.thr * 1.001 + 1e-30;
             const uint32_t j = s0 + tid;
             if (j < j1) {
                 const double4 p = P[j];
                 const double s2 = dmul(p.w, p.w);
                 s_src[tid] = make_double4(p.x, p.y, p.z, dmul(10.0, s2));
-                s_rs[tid] = ddiv(1.0, s2);
+                if (!far) s_rs[tid] = ddiv(1.0, s2);
             }
             __syncthreads();
             const int cnt = (int)min((uint32_t)kBsST, j1 - s0);
+            if (far) {
+                for (int jj = 0; jj < cnt; ++jj) {
+                    const double4 sj = s_src[jj];
+#pragma unroll
+                    for (int r = 0; r < kBsR; ++r) {
+                        const double dx = dsub(tx[r], sj.x);
+                        const double dz = dsub(tz[r], sj.y);
+                        const double K = __drcp_rn(dadd(dmul(dx, dx), dmul(dz, dz)));
+                        uu[r] = dsub(uu[r], dmul(dmul(K, dz), sj.z));
+                        ww[r] = dadd(ww[r], dmul(dmul(K, dx), sj.z));
+                    }
+                }
+                continue;
+            }
             for (int jj = 0; jj < cnt; ++jj) {
                 const double4 s = s_src[jj];
 #pragma unroll
@@ -644,7 +695,8 @@ __global__ void __launch_bounds__(kBsThreads, kF64Ctas)
     }
 }
 
-// Sum chunk partials in chunk order, scale by 1/(2 pi), scatter to blob order.
+// Per blob: the FP32 path's fixed-point sums, or the FP64 path's chunk partials
+// in chunk order; scale by 1/(2 pi), scatter to blob order.
 __global__ void k_self_combine(const InstDesc* __restrict__ table,
                                const InstState* __restrict__ st,
                                const ListEntry* __restrict__ list, int nlist,
@@ -670,16 +722,17 @@ __global__ void k_self_combine(const InstDesc* __restrict__ table,
         const uint32_t t = (item - s_pre[k]) * blockDim.x + threadIdx.x;
         if (t >= n) continue;
         double su = 0.0, sw = 0.0;
-        for (int c = 0; c < e.chunks; ++c) {
-            const double2 v = part[e.poff + (uint64_t)c * e.cap + t];
-            su += v.x;
-            sw += v.y;
-        }
-        if (macc) {  // what the mutual far tiles gave this blob as a source
+        if (macc) {  // FP32: the blob's fixed-point sums
             const double inv = ldexp(1.0, -mutual_shift(mexp, e.inst, n));
             const uint64_t g = 2 * (e.coff + t);
-            su += (double)(long long)macc[g] * inv;
-            sw -= (double)(long long)macc[g + 1] * inv;
+            su = (double)(long long)macc[g] * inv;
+            sw = (double)(long long)macc[g + 1] * inv;
+        } else {  // FP64: the chunk partials in chunk order
+            for (int c = 0; c < e.chunks; ++c) {
+                const double2 v = part[e.poff + (uint64_t)c * e.cap + t];
+                su += v.x;
+                sw += v.y;
+            }
         }
         const InstDesc& d = table[e.inst];
         const uint32_t p = perm ? perm[e.coff + t] : t;
@@ -1015,15 +1068,14 @@ size_t cub_sort_bytes(uint64_t total) {
 
 void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                          int precision, const Workspace& ws, int sms, cudaStream_t s) {
-    const uint32_t* perm = nullptr;
-    if (precision == kF32) {
+    {  // both precisions evaluate over Morton-sorted tiles
         const int g = (int)std::min<uint64_t>((ws.total_cap + 255) / 256, (uint64_t)sms * 16);
         k_keys<<<g, 256, 0, s>>>(table, st, list, nlist, ws.total_cap, ws.keys_in, ws.vals_in);
         size_t bytes = ws.cub_bytes;
         cub::DeviceRadixSort::SortPairs(ws.cub_tmp, bytes, ws.keys_in, ws.keys_out, ws.vals_in,
                                         ws.perm, (int64_t)ws.total_cap, 0, ws.key_bits, s);
-        perm = ws.perm;
     }
+    const uint32_t* perm = ws.perm;
     double2* pxz = precision == kF32 ? reinterpret_cast<double2*>(ws.packed) : nullptr;
     float4* pf = precision == kF32 ? reinterpret_cast<float4*>(ws.packed + ws.packed_cap / 2)
                                    : nullptr;
@@ -1043,19 +1095,19 @@ void biot_savart_compute(const InstDesc* table, InstState* st, const ListEntry* 
         const float4* pf = reinterpret_cast<const float4*>(ws.packed + ws.packed_cap / 2);
         const int g = sms * std::max(1, std::min(cfg.ctas, kSelfMinBlocks));
         cudaMemsetAsync(ws.macc, 0, 16 * ws.total_cap, s);
-        k_self_f32<kSelfMinBlocks><<<g, 32 * kWWarps, 0, s>>>(
-            st, list, nlist, pxz, pf, ws.meta, ws.part, ws.macc, ws.mexp, ws.work);
+        k_self_f32<kSelfMinBlocks><<<g, 32 * kWWarps, 0, s>>>(st, list, nlist, pxz, pf, ws.meta,
+                                                             ws.macc, ws.mexp, ws.work);
     } else {
-        k_self_f64<<<sms * kF64Ctas, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.part,
-                                                             ws.work);
+        k_self_f64<<<sms * kF64Ctas, kBsThreads, 0, s>>>(st, list, nlist, ws.packed, ws.meta,
+                                                             ws.part, ws.work);
     }
 }
 
 void biot_savart_finish(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
                         int precision, const Workspace& ws, int sms, cudaStream_t s) {
     const bool f32 = precision == kF32;
-    k_self_combine<<<sms * 8, 256, 0, s>>>(table, st, list, nlist, f32 ? ws.perm : nullptr,
-                                           ws.part, f32 ? ws.macc : nullptr, ws.mexp);
+    k_self_combine<<<sms * 8, 256, 0, s>>>(table, st, list, nlist, ws.perm, ws.part,
+                                           f32 ? ws.macc : nullptr, ws.mexp);
 }
 
 void biot_savart_self(const InstDesc* table, InstState* st, const ListEntry* list, int nlist,
