@@ -403,6 +403,29 @@ def run_rhs(n: int, npanels: int, reps: int, seed: int = 2):
             "fp32_peak_frac": tf / _fp32_peak_tflops(sms)}
 
 
+def run_setup(panels=(64, 128, 256, 512, 1024), reps: int = 5):
+    """Per-body set-up (src/VortexSheet.cpp:78-165 plus the factorisation that
+    replaces the per-step LAPACK solve): wall time of creating a simulation on a
+    circle of np panels -- geometry, uploads, influence matrix, QR, P -- best of
+    `reps` after one warm-up creation."""
+    import time
+    ctx = N.Context(0)
+    out = {"workload": "setup", "reps": reps, "ms": {}}
+    for npan in panels:
+        bx, bz = W.circle(npan)
+        ctx.sim(N.Params(capacity=1024), bx, bz).close()
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            sim = ctx.sim(N.Params(capacity=1024), bx, bz)
+            ctx.sync()
+            best = min(best, time.perf_counter() - t0)
+            sim.close()
+        out["ms"][str(npan)] = best * 1e3
+    ctx.close()
+    return out
+
+
 def run_book(n: int, npanels: int, inside: float, reps: int, seed: int = 3):
     """Bookkeeping phases alone on one simulation: a circle of npanels panels
     (R = 0.5) and n blobs, a fraction `inside` of them inside the body, the rest
@@ -483,6 +506,8 @@ def main(argv=None):
     rh.add_argument("--n", type=int, default=1 << 17)
     rh.add_argument("--panels", type=int, default=1024)
     rh.add_argument("--reps", type=int, default=3)
+    su = sub.add_parser("setup")
+    su.add_argument("--reps", type=int, default=5)
     pr = sub.add_parser("precision")
     pr.add_argument("--steps", type=int, default=20)
     pr.add_argument("--n-wake", type=int, default=1 << 19)
@@ -501,6 +526,8 @@ def main(argv=None):
                                      a.max_active, a.budget_gb, a.realtime or a.live, a.serial,
                                      not a.no_graph, not a.no_sync, a.autotune, a.live,
                                      serial_every=a.serial_every)))
+    if a.cmd == "setup":
+        print(json.dumps(run_setup(reps=a.reps)))
     if a.cmd == "sheet":
         print(json.dumps(run_sheet(a.n, a.panels, a.reps)))
     if a.cmd == "book":

@@ -97,7 +97,7 @@ def test_empty_blob_solve(ctx, port):
     s.close()
 
 
-@pytest.mark.parametrize("npanels", [40, 300, 700, 1100])
+@pytest.mark.parametrize("npanels", [13, 40, 300, 700, 1100])
 def test_pseudo_inverse_every_kernel_path(ctx, npanels):
     """The once-per-body factorisation has a register-resident path per column
     length (m = np + 1 <= 288, 544, 1056) and a general path above that; each
