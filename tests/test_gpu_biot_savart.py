@@ -103,6 +103,20 @@ def test_self_f32_vs_oracle(ctx, port, n):
     assert rel_l2(w, w0) <= F32_REL_L2, rel_l2(w, w0)
 
 
+def test_f32_edge_magnitudes(ctx, port):
+    """Range edges of the fixed-point sums: no circulation anywhere gives exact
+    zeros (the shift clamps); zero core sizes (every pair on the 1/r^2 branch,
+    as the reference's test r2 < 10 sigma^2 then never holds) and mixed core
+    sizes over three decades match the oracle."""
+    x, z, g, s = W.wake(5000, 31, 0.0818804)
+    u, w = ctx.biot_savart_self(x, z, np.zeros_like(g), s, N.F32)
+    assert np.all(u == 0.0) and np.all(w == 0.0)
+    for sig in (np.zeros_like(s), np.exp(np.random.default_rng(4).uniform(-7.0, -0.5, s.size))):
+        u0, w0 = port.direct_self(x, z, g, sig)
+        u, w = ctx.biot_savart_self(x, z, g, sig, N.F32)
+        assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
+
+
 def test_self_f32_clustered_boundary_layer(ctx, port):
     """Dense nascent-blob layer next to a body: close pairs dominate."""
     rng = np.random.default_rng(3)
