@@ -385,8 +385,11 @@ __device__ __forceinline__ float core_kernel_expm1(float r2, float rs, float rcp
     return r2 > 1e-30f ? -e * rcp_r2 : rs;
 }
 
-// One staged source against the warp's targets with the exact core test.
-template <int WP>
+// One staged source against the warp's targets with the exact core test.  SELF
+// (the target tile's own sources): a pair at r2 == 0 adds nothing, which is the
+// reference's i != j skip for the self pair whatever the core size (sigma = 0
+// would otherwise give 1/0 times dz = 0).
+template <int WP, bool SELF>
 __device__ __forceinline__ void near_pair(uint64_t sx, uint64_t sz, uint64_t sg, float2 C,
                                           const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                           uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
@@ -403,6 +406,10 @@ __device__ __forceinline__ void near_pair(uint64_t sx, uint64_t sz, uint64_t sg,
             ka = ca ? qa : ka;
             kb = cb ? qb : kb;
         }
+        if (SELF) {
+            ka = ra > 0.0f ? ka : 0.0f;
+            kb = rb > 0.0f ? kb : 0.0f;
+        }
         const uint64_t g = f2mul(f2pack(ka, kb), sg);
         nu2[q] = f2fma(g, dz, nu2[q]);
         w2[q] = f2fma(g, dx, w2[q]);
@@ -415,7 +422,7 @@ __device__ __forceinline__ void near_pair(uint64_t sx, uint64_t sz, uint64_t sg,
 // runs for both halves of a packed pair, branch-free, whenever any lane of the
 // warp has a pair inside the core, and a select keeps it only for those pairs,
 // so a pair's value does not depend on its neighbours in the warp.
-template <int WP>
+template <int WP, bool SELF>
 __device__ __forceinline__ void stage_near(const StagedTile& __restrict__ src,
                                            const uint64_t (&tx2)[WP], const uint64_t (&tz2)[WP],
                                            uint64_t (&nu2)[WP], uint64_t (&w2)[WP]) {
@@ -424,8 +431,10 @@ __device__ __forceinline__ void stage_near(const StagedTile& __restrict__ src,
         const float4 P = src.pos2[i];
         const float4 G = src.gam2[i];
         const float2 C0 = src.core[2 * i], C1 = src.core[2 * i + 1];
-        near_pair(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), C0, tx2, tz2, nu2, w2);
-        near_pair(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), C1, tx2, tz2, nu2, w2);
+        near_pair<WP, SELF>(f2pack(P.x, P.x), f2pack(P.y, P.y), f2pack(G.x, G.y), C0, tx2, tz2,
+                            nu2, w2);
+        near_pair<WP, SELF>(f2pack(P.z, P.z), f2pack(P.w, P.w), f2pack(G.z, G.w), C1, tx2, tz2,
+                            nu2, w2);
     }
 }
 
@@ -557,8 +566,10 @@ __global__ void __launch_bounds__(32 * kWWarps, MINB)
                              min((uint32_t)kBsST, j1 - s0), scale, lane);
             } else if (g2 > m.thr * 1.001 + 1e-30) {
                 stage_far(wsrc, tx2, tz2, nu2, w2);
+            } else if (s0 == t0) {
+                stage_near<kWP, true>(wsrc, tx2, tz2, nu2, w2);
             } else {
-                stage_near(wsrc, tx2, tz2, nu2, w2);
+                stage_near<kWP, false>(wsrc, tx2, tz2, nu2, w2);
             }
 #pragma unroll
             for (int q = 0; q < kWP; ++q) {  // Kahan fold of the stage partials
