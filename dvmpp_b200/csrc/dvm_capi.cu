@@ -343,7 +343,7 @@ int ensure_workspace(dvm_ctx* c, uint64_t cap, uint64_t part, uint64_t rhs, uint
     const size_t o_keys_in = take(8 * cap), o_keys_out = take(8 * cap), o_vals = take(4 * cap),
                  o_perm = take(4 * cap), o_packed = take(32 * cap),
                  o_meta = take(sizeof(TileMeta) * (cap / kBsST + 1)), o_part = take(16 * part),
-                 o_macc = take(16 * cap), o_mexp = take(sizeof(int) * 2 * kTableCap),
+                 o_macc = take(16 * cap), o_mexp = take(sizeof(int) * 4 * kTableCap),
                  o_rhs = take(16 * rhs), o_circ = take(8 * circ + 8), o_cub = take(cub + 256),
                  o_work = take(64 * sizeof(unsigned)), o_flags = take(cap),
                  o_tiles = take(4 * (cap / 1024 + 1)),

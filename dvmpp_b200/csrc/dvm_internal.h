@@ -156,8 +156,9 @@ struct Workspace {
     double2* part = nullptr;       // N-body partials
     // FP32 N-body, mutual far tiles: per sorted blob two 64-bit fixed-point sums
     // (Gamma_i K dz, Gamma_i K dx over the targets i whose tile evaluated this blob as a
-    // source), 2 * total_cap; and per simulation slot the two exponent bounds of
-    // their scale (2 * kTableCap)
+    // source), 2 * total_cap; and per simulation slot the exponent bounds of
+    // their scale (max |Gamma|, 1 / min core radius, max |coordinate|, one unused:
+    // 4 * kTableCap)
     unsigned long long* macc = nullptr;
     int* mexp = nullptr;
     double2* rhs_part = nullptr;   // at-target partials

