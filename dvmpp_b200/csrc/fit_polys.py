@@ -1,7 +1,8 @@
-"""Coefficients of the polynomial evaluations in the FP32 sheet-on-blob
-kernel (k_sheet.cu, sheet_pair_f32): fitted here, pasted there.
+"""Coefficients of the polynomial evaluations in the FP32 kernels: the
+sheet-on-blob kernel (k_sheet.cu, sheet_pair_f32) and the blob-on-blob core
+kernel (k_biot_savart.cu, core_kernel): fitted here, pasted there.
 
-    python dvmpp_b200/csrc/fit_sheet_polys.py
+    python dvmpp_b200/csrc/fit_polys.py
 
 Method: Lawson's algorithm (C. L. Lawson, 1961) -- iteratively reweighted
 least squares on a dense Chebyshev grid, which converges to the minimax
@@ -11,6 +12,9 @@ least squares on a dense Chebyshev grid, which converges to the minimax
   T(s) ~ atan(t) / t, s = t^2 on t in [0, 1/4],    degree 3 in s (small angles)
   G(s) ~ atan(t) / t, s = t^2 on t in [0, 1],      degree 9 in s (any angle,
                                                    after |t| = min / max)
+  P(t) ~ (1 - exp(-t)) / t  on t in [0, 1/2],       degree 5 in t (the
+                                                   regularised core below
+                                                   t = r^2 / sigma^2 = 1/2)
 
 Each fit prints its coefficients (constant term first) and the maximum
 relative error of the FP32 Horner evaluation (numpy float32, fused
@@ -75,6 +79,12 @@ def main():
     ts = np.linspace(1e-6, 1.0, 400001)
     report("G (atan, |t| <= 1)", c, np.arctan, ts, lambda t: t.astype(np.float64) ** 2,
            lambda t, p: (t.astype(np.float64) * p.astype(np.float64)).astype(np.float32))
+
+    # (1 - exp(-t)) / t on 0 <= t <= 1/2 (the value at t = 0 is 1)
+    h = lambda t: np.where(t == 0, 1.0, -np.expm1(-t) / np.where(t == 0, 1.0, t))
+    c = lawson(h, 0.0, 0.5, 5)
+    ts = np.linspace(0.0, 0.5, 200001)
+    report("P (core, t <= 1/2)", c, h, ts, lambda t: t, lambda t, p: p)
 
 
 if __name__ == "__main__":

@@ -360,22 +360,22 @@ __device__ __forceinline__ void stage_mutual(const StagedTile& __restrict__ src,
 
 // Core kernel (1 - exp(-r2/sigma^2)) / r2 in FP32, written as rs phi(t) with
 // t = r2 rs, rs = 1/sigma^2 and phi(t) = (1 - e^-t) / t.  For t < 1/2 phi is
-// its Taylor series sum_k (-t)^k / (k+1)! to degree 8 (truncation below 6e-10
-// relative, and phi(0) = 1 gives the r -> 0 limit 1/sigma^2: the self pair
-// then contributes exactly zero, as the reference's i != j skip gives, and
-// distinct blobs closer than FP32 resolves stay finite, as the FP64 reference
-// is).  For t >= 1/2 it is (1 - e) / r2 with e = 2^(-t log2 e) from one MUFU
-// ex2; 1 - e >= 0.39 there, so the ex2 error stays below 4e-7 relative.
+// a degree-5 polynomial, minimax in relative error on [0, 1/2] (Lawson's
+// algorithm, csrc/fit_polys.py: 6.1e-8 relative in FP32 Horner form, the
+// degree-8 Taylor series it replaced gave 6.5e-8 with three more FMAs per
+// half).  Its constant term 1 = phi(0) gives the r -> 0 limit 1/sigma^2: the
+// self pair then contributes exactly zero, as the reference's i != j skip
+// gives, and distinct blobs closer than FP32 resolves stay finite, as the
+// FP64 reference is.  For t >= 1/2 it is (1 - e) / r2 with e = 2^(-t log2 e)
+// from one MUFU ex2; 1 - e >= 0.39 there, so the ex2 error stays below 4e-7
+// relative.
 __device__ __forceinline__ float core_kernel(float r2, float rs, float rcp_r2) {
     const float t = r2 * rs;
-    float p = 1.0f / 362880.0f;
-    p = fmaf(p, t, -1.0f / 40320.0f);
-    p = fmaf(p, t, 1.0f / 5040.0f);
-    p = fmaf(p, t, -1.0f / 720.0f);
-    p = fmaf(p, t, 1.0f / 120.0f);
-    p = fmaf(p, t, -1.0f / 24.0f);
-    p = fmaf(p, t, 1.0f / 6.0f);
-    p = fmaf(p, t, -0.5f);
+    float p = -1.121634850e-03f;
+    p = fmaf(p, t, 8.187386207e-03f);
+    p = fmaf(p, t, -4.162909091e-02f);
+    p = fmaf(p, t, 1.666622460e-01f);
+    p = fmaf(p, t, -4.999998212e-01f);
     p = fmaf(p, t, 1.0f);
     const float e = ex2_approx(-t * 1.44269504088896341f);
     return t < 0.5f ? rs * p : (1.0f - e) * rcp_r2;

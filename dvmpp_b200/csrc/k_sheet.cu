@@ -404,7 +404,7 @@ __global__ void k_residual(const InstDesc* __restrict__ table, const ListEntry* 
 // this grouping keeps FP32 rounding relative to the result (the FP64
 // instances keep the reference's grouping).
 
-// Coefficients from dvmpp_b200/csrc/fit_sheet_polys.py (Lawson's algorithm,
+// Coefficients from dvmpp_b200/csrc/fit_polys.py (Lawson's algorithm,
 // minimax relative error; each FP32 Horner evaluation is within 1.8e-7 of the
 // function, relative).
 // atan2(y, x) for any quadrant: q = min(|x|, |y|) / max(|x|, |y|) in [0, 1],
