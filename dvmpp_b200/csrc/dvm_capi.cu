@@ -979,12 +979,15 @@ int dvm_sim_bytes(const dvm_sim_params* p, int np, uint64_t* bytes) {
     return DVM_OK;
 }
 
-int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const double* bz,
-                   int npts, dvm_sim** out) {
-    if (!p || !bx || !bz || !out) return fail(DVM_ERR_ARG, "null argument");
-    *out = nullptr;
-    // the body and the parameters are checked before the context, so a caller
-    // (or a test without a GPU) learns about a bad contour from its message
+}  // extern "C"
+
+namespace {
+
+// The checks of a simulation's parameters and body, made before anything
+// touches a device, so a caller (or a test without a GPU) learns about a bad
+// contour from its message.
+int check_sim_args(const dvm_sim_params* p, const double* bx, const double* bz, int npts) {
+    if (!p || !bx || !bz) return fail(DVM_ERR_ARG, "null argument");
     if (npts < 0) return fail(DVM_ERR_ARG, "negative point count");
     const std::string why = body_problem(bx, bz, npts);
     if (!why.empty()) return fail(DVM_ERR_ARG, why);
@@ -997,25 +1000,24 @@ int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const 
     if (p->rng != DVM_RNG_INJECT && p->rng != DVM_RNG_PHILOX) return fail(DVM_ERR_ARG, "bad rng");
     if (!(p->dt > 0) || !(p->nu > 0) || !(p->rho > 0)) return fail(DVM_ERR_ARG, "dt, nu, density must be > 0");
     if (p->capacity == 0 || p->capacity > 0xF0000000ull) return fail(DVM_ERR_ARG, "bad capacity");
+    if (npts - 1 > 2048) return fail(DVM_ERR_ARG, "too many panels (max 2048)");
+    return DVM_OK;
+}
+
+uint64_t setup_scratch_bytes(int np) {
+    return 8 * (2 * (uint64_t)np * np + pseudo_inverse_work_doubles(np));
+}
+
+// One simulation's set-up, enqueued on the context's stream up to its
+// factorisation: slab, descriptor, host geometry and panel tables, uploads and
+// the influence matrix; *scratch receives the factorisation's workspace.
+int begin_sim(dvm_ctx* c, int slot, const dvm_sim_params* p, const double* bx, const double* bz,
+              int npts, dvm_sim** out, double** scratch) {
     const int np = npts - 1;
-    if (np > 2048) return fail(DVM_ERR_ARG, "too many panels (max 2048)");
-    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
-    std::lock_guard<std::mutex> lk(c->mu);
-    int slot = -1;
-    for (int i = 1; i < kTableCap; ++i)  // slot 0 is the plugin-call scratch
-        if (!c->slots[i]) {
-            slot = i;
-            break;
-        }
-    if (slot < 0) return fail(DVM_ERR_OOM, "simulation table full");
-    CK(cudaSetDevice(c->device));
     const uint64_t cap = align_up(p->capacity, kCapAlign);
     std::vector<size_t> offs;
     const uint64_t bytes = sim_layout(p, np, cap, &offs);
-    const uint64_t qr_bytes = 8 * (2 * (size_t)np * np + pseudo_inverse_work_doubles(np));
-    if (c->in_use + bytes + qr_bytes > c->budget)
-        return fail(DVM_ERR_OOM, "simulation of " + std::to_string(bytes) +
-                                     " B does not fit the HBM budget");
+    const uint64_t qr_bytes = setup_scratch_bytes(np);
     auto* s = new dvm_sim();
     s->ctx = c;
     s->slot = slot;
@@ -1112,31 +1114,123 @@ int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const 
     if (e == cudaSuccess) e = up(s2, vs2.data(), np);
     if (e == cudaSuccess) e = up(psig, vps.data(), np);
     if (e == cudaSuccess) e = cudaMemsetAsync(h.gamma, 0, 8 * np, c->stream);
-    // influence matrix and pseudo-inverse, once per body
-    double* scratch = nullptr;
-    if (e == cudaSuccess) e = pool_alloc(c, reinterpret_cast<void**>(&scratch), qr_bytes);
-    if (e == cudaSuccess) {
-        influence_matrix(xp, zp, xc, zc, ds, th, np, scratch, A, c->stream);
-        e = pseudo_inverse(A, np, P, scratch, c->stream);
-        g_launches += 2 + 1 + 1 + 1 + 1;
-        const cudaError_t e2 = cudaStreamSynchronize(c->stream);
-        if (e == cudaSuccess) e = e2;
-    }
-    pool_free(c, scratch);
-    InstState st0;
-    std::memset(&st0, 0, sizeof(st0));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_state + slot, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(c->d_table + slot, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = pool_alloc(c, reinterpret_cast<void**>(scratch), qr_bytes);
+    if (e == cudaSuccess) influence_matrix(xp, zp, xc, zc, ds, th, np, *scratch, A, c->stream);
     if (e != cudaSuccess) {
+        pool_free(c, *scratch);
+        *scratch = nullptr;
         pool_free(c, s->slab);
         delete s;
         return fail(DVM_ERR_CUDA, std::string("sim create: ") + cudaGetErrorString(e));
     }
-    c->slots[slot] = s;
-    c->in_use += bytes;
     *out = s;
     return DVM_OK;
+}
+
+// Creates n simulations (all or none).  Their set-up is enqueued body after
+// body; the factorisations of the bodies then run together (pseudo_inverse_many:
+// up to 8 bodies per cooperative launch, the same arithmetic as alone), and one
+// wait covers them all.
+int create_sims(dvm_ctx* c, int n, const dvm_sim_params* const* p, const double* const* bx,
+                const double* const* bz, const int* npts, dvm_sim** out) {
+    for (int i = 0; i < n; ++i) out[i] = nullptr;
+    for (int i = 0; i < n; ++i) {
+        const int rc = check_sim_args(p[i], bx[i], bz[i], npts[i]);
+        if (rc && n > 1) return fail(rc, "simulation " + std::to_string(i) + ": " + g_err);
+        if (rc) return rc;
+    }
+    if (!c) return fail(DVM_ERR_ARG, "ctx is null");
+    std::lock_guard<std::mutex> lk(c->mu);
+    std::vector<int> slots;
+    for (int i = 1; i < kTableCap && (int)slots.size() < n; ++i)  // slot 0: plugin-call scratch
+        if (!c->slots[i]) slots.push_back(i);
+    if ((int)slots.size() < n) return fail(DVM_ERR_OOM, "simulation table full");
+    CK(cudaSetDevice(c->device));
+    uint64_t need = 0, bytes0 = 0;
+    for (int i = 0; i < n; ++i) {
+        const int np = npts[i] - 1;
+        const uint64_t cap = align_up(p[i]->capacity, kCapAlign);
+        const uint64_t bytes = sim_layout(p[i], np, cap, nullptr);
+        if (i == 0) bytes0 = bytes;
+        need += bytes + setup_scratch_bytes(np);  // the scratch is freed once set up
+    }
+    if (c->in_use + need > c->budget)
+        return fail(DVM_ERR_OOM, n == 1 ? "simulation of " + std::to_string(bytes0) +
+                                              " B does not fit the HBM budget"
+                                        : std::to_string(n) + " simulations with their set-up (" +
+                                              std::to_string(need) +
+                                              " B) do not fit the HBM budget");
+    std::vector<dvm_sim*> sims(n, nullptr);
+    std::vector<double*> scratch(n, nullptr);
+    auto abandon = [&](int rc) {  // nothing of the group is registered
+        for (int i = 0; i < n; ++i) {
+            pool_free(c, scratch[i]);
+            if (sims[i]) {
+                pool_free(c, sims[i]->slab);
+                delete sims[i];
+            }
+        }
+        return rc;
+    };
+    for (int i = 0; i < n; ++i) {
+        const int rc = begin_sim(c, slots[i], p[i], bx[i], bz[i], npts[i], &sims[i], &scratch[i]);
+        if (rc) return abandon(rc);
+    }
+    // influence matrices are enqueued; the factorisations, once per body
+    std::vector<const double*> A(n);
+    std::vector<double*> P(n);
+    std::vector<int> np(n);
+    for (int i = 0; i < n; ++i) {
+        A[i] = sims[i]->h.A;
+        P[i] = const_cast<double*>(sims[i]->h.P);  // the slab is ours; kernels read it const
+        np[i] = sims[i]->h.np;
+    }
+    int launches = 0;
+    cudaError_t e = pseudo_inverse_many(n, A.data(), np.data(), P.data(), scratch.data(),
+                                        c->stream, &launches);
+    g_launches += 3 * (uint64_t)n + (uint64_t)launches;  // influence matrix 2, load 1 per body
+    const cudaError_t e2 = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = e2;
+    for (int i = 0; i < n; ++i) {
+        pool_free(c, scratch[i]);
+        scratch[i] = nullptr;
+    }
+    InstState st0;
+    std::memset(&st0, 0, sizeof(st0));
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        const int slot = sims[i]->slot;
+        e = cudaMemcpyAsync(c->d_state + slot, &st0, sizeof(st0), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->d_table + slot, &sims[i]->h, sizeof(InstDesc),
+                                cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess)
+        return abandon(fail(DVM_ERR_CUDA, std::string("sim create: ") + cudaGetErrorString(e)));
+    for (int i = 0; i < n; ++i) {
+        c->slots[sims[i]->slot] = sims[i];
+        c->in_use += sims[i]->bytes;
+        out[i] = sims[i];
+    }
+    return DVM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dvm_sim_create(dvm_ctx* c, const dvm_sim_params* p, const double* bx, const double* bz,
+                   int npts, dvm_sim** out) {
+    if (!p || !bx || !bz || !out) return fail(DVM_ERR_ARG, "null argument");
+    return create_sims(c, 1, &p, &bx, &bz, &npts, out);
+}
+
+int dvm_sims_create(dvm_ctx* c, int n, const dvm_sim_params* const* p, const double* const* bx,
+                    const double* const* bz, const int* npts, dvm_sim** out) {
+    if (n < 0 || (n > 0 && (!p || !bx || !bz || !npts || !out)))
+        return fail(DVM_ERR_ARG, "bad argument");
+    if (n == 0) return DVM_OK;
+    return create_sims(c, n, p, bx, bz, npts, out);
 }
 
 int dvm_sim_destroy(dvm_sim* s) {

@@ -276,8 +276,14 @@ void step_counter(InstState* st, const ListEntry* list, int nlist, cudaStream_t 
 void influence_matrix(const double* xp, const double* zp, const double* xc, const double* zc,
                       const double* ds, const double* theta, int np, double* pq_scratch,
                       double* A, cudaStream_t s);
-// Householder QR of A ((np+1) x np, row-major) and P = R^-1 Q^T (np x (np+1)).
-cudaError_t pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s);
+// Householder QR of A ((np+1) x np, row-major) and P = R^-1 Q^T (np x (np+1))
+// for n bodies, each with its own A, P and workspace
+// (pseudo_inverse_work_doubles(np)): bodies that take the register-resident
+// path are factorised together, up to 8 per cooperative launch, with the same
+// arithmetic per body as alone.  *launches (if not null) receives the number of
+// factorisation kernels launched.
+cudaError_t pseudo_inverse_many(int n, const double* const* A, const int* np, double* const* P,
+                                double* const* work, cudaStream_t s, int* launches);
 size_t pseudo_inverse_work_doubles(int np);
 
 }  // namespace dvmk

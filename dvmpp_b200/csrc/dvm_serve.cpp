@@ -268,8 +268,46 @@ int dvm_server_run(dvm_server* s, int serial, int realtime) {
                            [&] { return !s->intake.empty() || s->intake_closed; });
             continue;
         }
-        // admission: FIFO while a slot is free and the slab fits the budget
+        // admission: FIFO while a slot is free and the slab fits the budget.  The
+        // requests that fit now are created together (their bodies' factorisations
+        // share launches); if that fails, the loop below takes them one at a time,
+        // so a request that cannot be created fails alone.
         const double ta = now();
+        {
+            std::vector<Request*> group;
+            uint64_t group_bytes = 0;
+            for (Request* r : waiting) {
+                if ((int)(active.size() + group.size()) >= cap_active) break;
+                if (in_use + group_bytes + r->bytes > s->budget) break;
+                group.push_back(r);
+                group_bytes += r->bytes;
+            }
+            if (group.size() > 1) {
+                const size_t g = group.size();
+                std::vector<const dvm_sim_params*> ps(g);
+                std::vector<const double*> xs(g), zs(g);
+                std::vector<int> npts(g);
+                std::vector<dvm_sim*> sims(g, nullptr);
+                for (size_t k = 0; k < g; ++k) {
+                    ps[k] = &group[k]->p;
+                    xs[k] = group[k]->bx.data();
+                    zs[k] = group[k]->bz.data();
+                    npts[k] = (int)group[k]->bx.size();
+                }
+                if (dvm_sims_create(s->ctx, (int)g, ps.data(), xs.data(), zs.data(), npts.data(),
+                                    sims.data()) == DVM_OK) {
+                    const double t_adm = now();
+                    std::lock_guard<std::mutex> lk(s->mu);
+                    for (size_t k = 0; k < g; ++k) {
+                        waiting.pop_front();
+                        group[k]->sim = sims[k];
+                        group[k]->admitted = t_adm;
+                        in_use += group[k]->bytes;
+                        active.push_back(group[k]);
+                    }
+                }
+            }
+        }
         while (!waiting.empty() && (int)active.size() < cap_active) {
             Request& r = *waiting.front();
             if (in_use + r.bytes > s->budget) break;

@@ -15,9 +15,11 @@
 // gamma = P b (a batched GEMV) plus one iterative-refinement step with the FP64
 // residual r = b - A gamma (gamma += P r).  Same least-squares solution, no
 // O(np^3) work per step.
+#include <algorithm>
 #include <cfloat>
 
 #include <cooperative_groups.h>
+#include <vector>
 
 #include "dvm_device.cuh"
 #include "dvm_internal.h"
@@ -223,21 +225,55 @@ __device__ __forceinline__ void house_reg(double (&x)[CH], int m, int k,
     }
 }
 
+// Bodies factorised together in one register-resident launch: bodies of one
+// register class share its grid barriers, so k bodies cost about as much as one
+// (a step is barrier-bound: ~1.2 us of a ~2 us step at np = 512).  Block b
+// belongs to the last body whose qr_block0 (k_qr_reg) or bs_block0
+// (k_backsub_reg) is <= b; a body's arithmetic does not depend on the others.
+constexpr int kQrMaxBodies = 8;
+struct QrBody {
+    double* M;
+    double* vbuf;
+    double* v0s;
+    double* taus;
+    double* P;
+    int np;
+    int qr_block0;
+    int bs_block0;
+};
+struct QrGroup {
+    QrBody b[kQrMaxBodies];
+    int nb;
+    int maxnp;
+};
+
+__device__ __forceinline__ int qr_body_of(const QrGroup& G, bool backsub) {
+    int k = 0;
+    while (k + 1 < G.nb &&
+           (int)blockIdx.x >= (backsub ? G.b[k + 1].bs_block0 : G.b[k + 1].qr_block0))
+        ++k;
+    return k;
+}
+
 // Register-resident variant for m <= 32 CH: one warp owns one column of the
 // augmented [A | I] for the whole factorisation (CH values per lane), so a step
 // reads only the reflector from memory.  Step k: every warp with a column
 // c > k applies H_k; the warp owning column k+1 then forms reflector k+1 from
 // its registers (double-buffered v).  The identity columns become Q^T in
-// place.  At the end each warp stores its column of M.
+// place.  At the end each warp stores its column of M.  Every block takes the
+// group's maxnp - 1 grid barriers; a body's steps end at its own np.
 template <int CH>
-__global__ void __launch_bounds__(256, 2) k_qr_reg(double* __restrict__ M, int np,
-                                                double* __restrict__ vbuf,
-                                                double* __restrict__ v0s,
-                                                double* __restrict__ taus) {
+__global__ void __launch_bounds__(256, 2) k_qr_reg(const __grid_constant__ QrGroup G) {
     cg::grid_group grid = cg::this_grid();
+    const QrBody& B = G.b[qr_body_of(G, false)];
+    double* __restrict__ M = B.M;
+    double* __restrict__ vbuf = B.vbuf;
+    double* __restrict__ v0s = B.v0s;
+    double* __restrict__ taus = B.taus;
+    const int np = B.np;
     const int m = np + 1, cols = np + m;
     const int lane = threadIdx.x & 31;
-    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int c = (int)(((blockIdx.x - B.qr_block0) * blockDim.x + threadIdx.x) >> 5);
     const bool own = c < cols;
     double x[CH];
 #pragma unroll
@@ -248,8 +284,8 @@ __global__ void __launch_bounds__(256, 2) k_qr_reg(double* __restrict__ M, int n
     }
     if (c == 0) house_reg<CH>(x, m, 0, vbuf, v0s, taus, lane);
     grid.sync();
-    for (int k = 0; k < np; ++k) {
-        if (own && c > k) {
+    for (int k = 0; k < G.maxnp; ++k) {
+        if (k < np && own && c > k) {
             const double* v = vbuf + (size_t)(k & 1) * m;  // zero above row k
             double acc = 0.0;
 #pragma unroll
@@ -266,7 +302,7 @@ __global__ void __launch_bounds__(256, 2) k_qr_reg(double* __restrict__ M, int n
             if (c == k + 1 && k + 1 < np)
                 house_reg<CH>(x, m, k + 1, vbuf + (size_t)((k + 1) & 1) * m, v0s, taus, lane);
         }
-        if (k + 1 < np) grid.sync();
+        if (k + 1 < G.maxnp) grid.sync();
     }
     if (own) {
 #pragma unroll
@@ -281,11 +317,14 @@ __global__ void __launch_bounds__(256, 2) k_qr_reg(double* __restrict__ M, int n
 // per column c, CH values per lane) and R's next column prefetched while the
 // current one is applied.
 template <int CH>
-__global__ void __launch_bounds__(256) k_backsub_reg(const double* __restrict__ M, int np,
-                                                     double* __restrict__ P) {
+__global__ void __launch_bounds__(256) k_backsub_reg(const __grid_constant__ QrGroup G) {
+    const QrBody& B = G.b[qr_body_of(G, true)];
+    const double* __restrict__ M = B.M;
+    double* __restrict__ P = B.P;
+    const int np = B.np;
     const int m = np + 1;
     const int lane = threadIdx.x & 31;
-    const int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int c = (int)(((blockIdx.x - B.bs_block0) * blockDim.x + threadIdx.x) >> 5);
     if (c >= m) return;
     const double* qt = M + (size_t)(np + c) * m;
     double y[CH], rc[CH];
@@ -837,36 +876,50 @@ size_t pseudo_inverse_work_doubles(int np) {
     return m * (np + m) + 2 * m + 2 * (size_t)np + 8;
 }
 
-cudaError_t pseudo_inverse(const double* A, int np, double* P, double* work, cudaStream_t s) {
+namespace {
+
+// A body's factorisation workspace: M = [A | I] (m x (np + m), column-major),
+// then the reflector buffer (2 m), v0s (np) and taus (np).
+QrBody qr_body(int np, double* P, double* work) {
     const int m = np + 1, cols = np + m;
-    double* M = work;
-    double* vbuf = M + (size_t)m * cols;
-    double* v0s = vbuf + 2 * (size_t)m;
-    double* taus = v0s + np;
-    k_load_aug<<<256, 256, 0, s>>>(A, np, M);
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // Register-resident path: one warp per column of [A | I], all resident.
-    auto reg_path = [&](auto kqr, auto kbs) -> int {
-        int per = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kqr, 256, 0);
-        const int blocks = (cols + 7) / 8;
-        if (blocks > per * sms) return 0;  // not co-resident: use the general path
-        void* args[] = {&M, &np, &vbuf, &v0s, &taus};
-        cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(kqr),
-                                                    dim3(blocks), dim3(256), args, 0, s);
-        if (e != cudaSuccess) return -1;
-        kbs<<<(m + 7) / 8, 256, 0, s>>>(M, np, P);
-        return 1;
-    };
-    int done = 0;
-    if (m <= 32 * 9) done = reg_path(k_qr_reg<9>, k_backsub_reg<9>);
-    else if (m <= 32 * 17) done = reg_path(k_qr_reg<17>, k_backsub_reg<17>);
-    else if (m <= 32 * 33) done = reg_path(k_qr_reg<33>, k_backsub_reg<33>);
-    if (done < 0) return cudaGetLastError();
-    if (done > 0) return cudaGetLastError();
-    // General path: one warp per column of A (columns in memory), then Q^T
+    QrBody b{};
+    b.M = work;
+    b.vbuf = b.M + (size_t)m * cols;
+    b.v0s = b.vbuf + 2 * (size_t)m;
+    b.taus = b.v0s + np;
+    b.P = P;
+    b.np = np;
+    return b;
+}
+
+// Register class of m rows: CH = 9, 17, 33 values per lane, or -1 (general path).
+int qr_class(int m) { return m <= 32 * 9 ? 0 : m <= 32 * 17 ? 1 : m <= 32 * 33 ? 2 : -1; }
+
+template <int CH>
+cudaError_t qr_group_launch(QrGroup& G, int qr_blocks, int bs_blocks, cudaStream_t s) {
+    void* args[] = {&G};
+    cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_qr_reg<CH>),
+                                                dim3(qr_blocks), dim3(256), args, 0, s);
+    if (e != cudaSuccess) return e;
+    k_backsub_reg<CH><<<bs_blocks, 256, 0, s>>>(G);
+    return cudaGetLastError();
+}
+
+cudaError_t qr_group_launch(int cls, QrGroup& G, int qr_blocks, int bs_blocks, cudaStream_t s) {
+    if (cls == 0) return qr_group_launch<9>(G, qr_blocks, bs_blocks, s);
+    if (cls == 1) return qr_group_launch<17>(G, qr_blocks, bs_blocks, s);
+    return qr_group_launch<33>(G, qr_blocks, bs_blocks, s);
+}
+
+// General path: one warp per column of A (columns in memory), then Q^T.
+cudaError_t qr_general(const QrBody& b, int sms, cudaStream_t s) {
+    double* M = b.M;
+    double* vbuf = b.vbuf;
+    double* v0s = b.v0s;
+    double* taus = b.taus;
+    int np = b.np;
+    const int m = np + 1;
+    int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qr_coop, 256, 0);
     const int blocks = std::max(1, std::min((np + 7) / 8, std::max(1, per_sm) * sms));
     void* args[] = {&M, &np, &vbuf, &v0s, &taus};
@@ -880,7 +933,64 @@ cudaError_t pseudo_inverse(const double* A, int np, double* P, double* work, cud
     else k_form_qt<65><<<g, 128, 0, s>>>(M, np, v0s, taus);  // np <= 2048
     // warps per block such that the per-warp right-hand sides fit 48 KB of shared memory
     const int wpb = std::max(1, std::min(4, (int)(48 * 1024 / (sizeof(double) * np))));
-    k_backsub<<<(m + wpb - 1) / wpb, wpb * 32, sizeof(double) * np * wpb, s>>>(M, np, P);
+    k_backsub<<<(m + wpb - 1) / wpb, wpb * 32, sizeof(double) * np * wpb, s>>>(M, np, b.P);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t pseudo_inverse_many(int n, const double* const* A, const int* np, double* const* P,
+                                double* const* work, cudaStream_t s, int* launches) {
+    int nl = 0;  // QR-stage launches (the loads of [A | I] are counted by the caller)
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per[3] = {0, 0, 0};  // co-resident register-path blocks per SM, by class
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_qr_reg<9>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_qr_reg<17>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_qr_reg<33>, 256, 0);
+    std::vector<QrBody> bodies(n);
+    std::vector<int> cls(n);
+    for (int i = 0; i < n; ++i) {
+        bodies[i] = qr_body(np[i], P[i], work[i]);
+        k_load_aug<<<256, 256, 0, s>>>(A[i], np[i], bodies[i].M);
+        const int m = np[i] + 1, c = qr_class(m);
+        // register path when one warp per column of [A | I] fits the GPU at once
+        cls[i] = (c >= 0 && (np[i] + m + 7) / 8 <= per[c] * sms) ? c : -1;
+    }
+    // Register path: bodies of a class in order, up to kQrMaxBodies per launch and
+    // as many as are co-resident together.
+    for (int c = 0; c < 3; ++c) {
+        QrGroup G{};
+        int qb = 0, bb = 0;
+        for (int i = 0; i <= n; ++i) {
+            const bool last = i == n;
+            if (!last && cls[i] != c) continue;
+            const int need = last ? 0 : (2 * np[i] + 1 + 7) / 8;
+            if (G.nb > 0 && (last || G.nb == kQrMaxBodies || qb + need > per[c] * sms)) {
+                const cudaError_t e = qr_group_launch(c, G, qb, bb, s);
+                if (e != cudaSuccess) return e;
+                nl += 2;
+                G = QrGroup{};
+                qb = bb = 0;
+            }
+            if (last) break;
+            QrBody b = bodies[i];
+            b.qr_block0 = qb;
+            b.bs_block0 = bb;
+            G.b[G.nb++] = b;
+            G.maxnp = std::max(G.maxnp, np[i]);
+            qb += need;
+            bb += (np[i] + 1 + 7) / 8;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        if (cls[i] >= 0) continue;
+        const cudaError_t e = qr_general(bodies[i], sms, s);
+        if (e != cudaSuccess) return e;
+        nl += 3;
+    }
+    if (launches) *launches = nl;
     return cudaGetLastError();
 }
 

@@ -82,6 +82,8 @@ SIGNATURES = {
     "dvm_biot_savart_at_noalloc": (C.c_int, [C.c_void_p] * 4 + [C.c_uint64] + [C.c_void_p] * 2
                                    + [C.c_uint64] + [C.c_void_p] * 2 + [C.c_int, C.c_int, C.c_void_p]),
     "dvm_sim_create": (C.c_int, [C.c_void_p, C.POINTER(SimParams), _dp, _dp, C.c_int, C.POINTER(C.c_void_p)]),
+    "dvm_sims_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.POINTER(SimParams)), C.POINTER(_dp),
+                                  C.POINTER(_dp), C.POINTER(C.c_int), C.POINTER(C.c_void_p)]),
     "dvm_sim_destroy": (C.c_int, [C.c_void_p]),
     "dvm_sim_set_blobs": (C.c_int, [C.c_void_p, C.c_uint64, _dp, _dp, _dp, _dp]),
     "dvm_sim_get_blobs": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)] + [_dp] * 8 + [_u32p]),
@@ -386,6 +388,29 @@ class Context:
 
     def sim(self, params: "Params", xp, zp) -> "Simulation":
         return Simulation(self, params, xp, zp)
+
+    def sims(self, params, bodies) -> list:
+        """Several simulations created together (dvm_sims_create): their bodies'
+        factorisations share launches.  params: one Params per body; bodies:
+        (x, z) contours.  All are created, or none (the error is raised)."""
+        n = len(bodies)
+        cps = [p.c() for p in params]
+        xs = [_f64(x) for x, _ in bodies]
+        zs = [_f64(z) for _, z in bodies]
+        pp = (C.POINTER(SimParams) * n)(*[C.pointer(cp) for cp in cps])
+        px = (_dp * n)(*[_p(x) for x in xs])
+        pz = (_dp * n)(*[_p(z) for z in zs])
+        npts = (C.c_int * n)(*[x.size for x in xs])
+        hs = (C.c_void_p * n)()
+        _check(self.lib.dvm_sims_create(self.h, n, pp, px, pz, npts, hs))
+        out = []
+        for k in range(n):
+            sim = Simulation.__new__(Simulation)
+            sim.ctx, sim.lib, sim.h = self, self.lib, C.c_void_p(hs[k])
+            sim.params = params[k]
+            sim.np = xs[k].size - 1
+            out.append(sim)
+        return out
 
     def restore(self, state: bytes, params: "Params" = None) -> "Simulation":
         """A simulation rebuilt from Simulation.save() output (in this context)."""

@@ -10,7 +10,8 @@
  * Reference interfaces replaced (gdeskos/DVMpp, file:line):
  *   dvm_biot_savart_self      DirectKernel::computeSelfInduced  src/VelocityKernel.cpp:30-67
  *   dvm_biot_savart_at        DirectKernel::computeInducedAt    src/VelocityKernel.cpp:69-109
- *   dvm_sim_create            VortexSheet(xml, stamp) set-up    src/VortexSheet.cpp:12-54,78-165
+ *   dvm_sim_create /
+ *   dvm_sims_create           VortexSheet(xml, stamp) set-up    src/VortexSheet.cpp:12-54,78-165
  *   dvm_sim_set_blobs /
  *   dvm_sim_get_blobs         VortexBlobs public SoA members    src/VortexBlobs.hpp:24-32
  *   dvm_sim_phase(BIOTSAVART) VortexBlobs::biotsavart           src/VortexBlobs.cpp:229-249
@@ -227,6 +228,17 @@ int dvm_biot_savart_at_noalloc(const double* x, const double* z, const double* c
  * the reference's domain_file format (src/VortexSheet.cpp:56-76). */
 int dvm_sim_create(dvm_ctx* ctx, const dvm_sim_params* p, const double* body_x,
                    const double* body_z, int npoints, dvm_sim** out);
+/* n simulations created together, as n calls of dvm_sim_create would create
+ * them (same set-up arithmetic, bit for bit), but the once-per-body QR
+ * factorisations of their influence matrices share cooperative launches (up to
+ * 8 bodies per launch) and one wait covers them all: a serving loop admitting
+ * several requests at once pays for about one factorisation chain instead of n.
+ * All or none: on any error no simulation is created and out[] stays NULL; an
+ * argument error names the offending index.  The reference builds one body per
+ * VortexSheet(xml, stamp) (src/VortexSheet.cpp:12-54,78-165). */
+int dvm_sims_create(dvm_ctx* ctx, int n, const dvm_sim_params* const* p,
+                    const double* const* body_x, const double* const* body_z,
+                    const int* npoints, dvm_sim** out);
 int dvm_sim_destroy(dvm_sim* sim);
 int dvm_sim_set_blobs(dvm_sim* sim, uint64_t n, const double* x, const double* z,
                       const double* circ, const double* sigma);

@@ -111,6 +111,43 @@ def test_pseudo_inverse_every_kernel_path(ctx, npanels):
     s.close()
 
 
+def test_group_created_sims_equal_alone(ctx):
+    """dvm_sims_create factorises the bodies of a group together (up to 8 per
+    cooperative launch per register class, the general path one by one); every
+    simulation's saved state, which holds A and P, must equal byte for byte the
+    same body created alone.  The group spans all three register classes,
+    more than 8 bodies of one class, and the general path (np = 1100)."""
+    panels = [13, 40, 64, 100, 150, 200, 250, 287, 64, 96, 300, 512, 543, 700, 1100]
+    bodies = [W.ellipse(n, a=0.5, b=0.5 / (1.0 + 0.2 * k), incidence_deg=3.0 * k)
+              for k, n in enumerate(panels)]
+    # two steps release up to 2 M np = 6 np blobs
+    ps = [params(capacity=max(4096, 8 * n), ux=1.0 + 0.1 * k, seed=k + 1)
+          for k, n in enumerate(panels)]
+    group = ctx.sims(ps, bodies)
+    for p, (bx, bz), g in zip(ps, bodies, group):
+        alone = ctx.sim(p, bx, bz)
+        assert g.save() == alone.save(), g.np
+        # and the two step alike
+        for s in (g, alone):
+            s.push_uniforms(np.random.default_rng(g.np).random(1 << 16))
+            s.step(2)
+            s.check()
+        assert g.save() == alone.save(), g.np
+        alone.close()
+        g.close()
+
+
+def test_group_create_is_all_or_nothing(ctx):
+    """One bad body (an open contour) fails the whole group with its index in
+    the message; nothing of the group stays allocated."""
+    used0, _ = ctx.memory()
+    good = W.circle(64)
+    bad = (good[0][:-1], good[1][:-1])  # last point not the first
+    with pytest.raises(Exception, match="simulation 2"):
+        ctx.sims([params(capacity=4096)] * 3, [good, good, bad])
+    assert ctx.memory()[0] == used0
+
+
 def test_diffusion_inject_matches(ctx, port):
     bx, bz = W.circle(64)
     p = params(nu=1e-3, dt=0.01)
