@@ -49,42 +49,61 @@ def horner_f32(c, v):
     return p
 
 
-def report(name, c, f, xs, var, post):
+def fitted(name, src, c, f, xs, var, post):
+    """The fit rounded to FP32 and its maximum relative error in FP32 Horner form."""
     c32 = [np.float32(v) for v in c]
     got = post(xs.astype(np.float32), horner_f32(c32, var(xs)))
     ref = f(xs)
-    err = np.max(np.abs(got.astype(np.float64) - ref) / np.abs(ref))
-    print(f"{name}: max rel err (FP32 Horner) {err:.3e}")
-    print("  " + ", ".join(f"{float(v):.9e}f" for v in c32))
+    err = float(np.max(np.abs(got.astype(np.float64) - ref) / np.abs(ref)))
+    return {"name": name, "source": src, "coefficients": c32, "max_rel_err": err}
 
 
-def main():
+def literal(v) -> str:
+    """A coefficient as the kernels spell it."""
+    return f"{float(v):.9e}f"
+
+
+def fits():
+    """Every polynomial: name, the kernel source it is pasted into, its FP32
+    coefficients (constant term first) and the error of its FP32 evaluation."""
+    out = []
     # log1p(x) = x * L(x), |x| <= 1/4
     f = lambda x: np.where(x == 0, 1.0, np.log1p(x) / np.where(x == 0, 1.0, x))
     c = lawson(f, -0.25, 0.25, 7)
     xs = np.linspace(-0.25, 0.25, 200001)
     xs = xs[xs != 0]
-    report("L (log1p, |x| <= 1/4)", c, lambda x: np.log1p(x), xs, lambda x: x,
-           lambda x, p: (x.astype(np.float64) * p.astype(np.float64)).astype(np.float32))
+    out.append(fitted("L (log1p, |x| <= 1/4)", "k_sheet.cu", c, lambda x: np.log1p(x), xs,
+                      lambda x: x,
+                      lambda x, p: (x.astype(np.float64) * p.astype(np.float64)).astype(np.float32)))
 
     # atan(t) = t * T(t^2), |t| <= 1/4
     g = lambda t: np.where(t == 0, 1.0, np.arctan(t) / np.where(t == 0, 1.0, t))
     c = lawson(lambda s: g(np.sqrt(s)), 0.0, 0.0625, 3)
     ts = np.linspace(1e-6, 0.25, 200001)
-    report("T (atan, |t| <= 1/4)", c, np.arctan, ts, lambda t: t.astype(np.float64) ** 2,
-           lambda t, p: (t.astype(np.float64) * p.astype(np.float64)).astype(np.float32))
+    out.append(fitted("T (atan, |t| <= 1/4)", "k_sheet.cu", c, np.arctan, ts,
+                      lambda t: t.astype(np.float64) ** 2,
+                      lambda t, p: (t.astype(np.float64) * p.astype(np.float64)).astype(np.float32)))
 
     # atan(t) = t * G(t^2), 0 <= t <= 1
     c = lawson(lambda s: g(np.sqrt(s)), 0.0, 1.0, 9)
     ts = np.linspace(1e-6, 1.0, 400001)
-    report("G (atan, |t| <= 1)", c, np.arctan, ts, lambda t: t.astype(np.float64) ** 2,
-           lambda t, p: (t.astype(np.float64) * p.astype(np.float64)).astype(np.float32))
+    out.append(fitted("G (atan, |t| <= 1)", "k_sheet.cu", c, np.arctan, ts,
+                      lambda t: t.astype(np.float64) ** 2,
+                      lambda t, p: (t.astype(np.float64) * p.astype(np.float64)).astype(np.float32)))
 
     # (1 - exp(-t)) / t on 0 <= t <= 1/2 (the value at t = 0 is 1)
     h = lambda t: np.where(t == 0, 1.0, -np.expm1(-t) / np.where(t == 0, 1.0, t))
     c = lawson(h, 0.0, 0.5, 5)
     ts = np.linspace(0.0, 0.5, 200001)
-    report("P (core, t <= 1/2)", c, h, ts, lambda t: t, lambda t, p: p)
+    out.append(fitted("P (core, t <= 1/2)", "k_biot_savart.cu", c, h, ts, lambda t: t,
+                      lambda t, p: p))
+    return out
+
+
+def main():
+    for r in fits():
+        print(f"{r['name']} ({r['source']}): max rel err (FP32 Horner) {r['max_rel_err']:.3e}")
+        print("  " + ", ".join(literal(v) for v in r["coefficients"]))
 
 
 if __name__ == "__main__":
