@@ -234,7 +234,10 @@ int dvm_sim_create(dvm_ctx* ctx, const dvm_sim_params* p, const double* body_x,
  * 8 bodies per launch) and one wait covers them all: a serving loop admitting
  * several requests at once pays for about one factorisation chain instead of n.
  * All or none: on any error no simulation is created and out[] stays NULL; an
- * argument error names the offending index.  The reference builds one body per
+ * argument error names the offending index.  The set-up scratch of all n
+ * bodies (about 32 np^2 bytes each) is held at once and counts against the
+ * budget (DVM_ERR_OOM if it does not fit); it returns to the pool before the
+ * call returns.  The reference builds one body per
  * VortexSheet(xml, stamp) (src/VortexSheet.cpp:12-54,78-165). */
 int dvm_sims_create(dvm_ctx* ctx, int n, const dvm_sim_params* const* p,
                     const double* const* body_x, const double* const* body_z,
