@@ -1,4 +1,4 @@
-"""The north-star configurations at their full sizes, as parity tests.
+"""The standalone N-body and sheet-solve workloads at their full sizes, as parity tests.
 
 Config 2 (standalone N-body, N = 2^20 wake + 256 collocation targets):
 DirectKernel::computeSelfInduced / computeInducedAt
